@@ -1,0 +1,311 @@
+"""ORACLE -- test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs
+import this module, and only as the checker (or as the timed CPU baseline).  The
+exmarg_b200 package never imports it.
+
+A restatement, in plain numpy plus the C gather of gather_fp64.c, of the
+reference's pe_intrinsic path.  Each function cites the reference code it follows.
+Two precisions:
+
+* precision='fp64': every step in float64 (filter FFT in complex128, the gather,
+  the cross-lag / node log-sum-exp and the distance quadrature) -- the all-FP64
+  oracle that gives the error of every result;
+* precision='ref': the filter in complex64 with float32 trajectories, exactly as
+  the reference's CPU path does (exmarg/search/bank.py:56-78), the rest as the
+  reference (float64 gather arithmetic over float32 inputs).
+
+Parity of this restatement with the reference itself is pinned by
+tests/test_oracle_golden.py against vectors produced by running the reference's
+own CPU code (tests/golden/make_golden.py).
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build_oracle
+
+NPHI = 96
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        lib = ctypes.CDLL(build_oracle.build())
+        P = ctypes.c_void_p
+        lib.oracle_gather.argtypes = [ctypes.c_int, P, P, P, P, ctypes.c_int, ctypes.c_int, P, P, P,
+                                      ctypes.c_int, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, P, P, ctypes.c_int, P]
+        lib.oracle_gather.restype = ctypes.c_int
+        lib.oracle_num_threads.restype = ctypes.c_int
+        _LIB = lib
+    return _LIB
+
+
+def num_threads():
+    return int(_lib().oracle_num_threads())
+
+
+# ----------------------------------------------------------------------------- segments
+
+def read_segments(segments, rows=None):
+    """exmarg/search/segments.py:11-37: d_H, d_L as complex128, sig2_H/L float64"""
+    z = np.load(segments) if isinstance(segments, (str, bytes, os.PathLike)) else segments
+    n = np.asarray(z["d_H"]).shape[0]
+    rows = np.arange(n) if rows is None else np.asarray(rows, int)
+    out = {"rows": rows, "f": np.asarray(z["f"], float), "nu": np.asarray(z["nu"], np.int64),
+           "T": float(z["T"]), "fmin": float(z["fmin"]), "fmax": float(z["fmax"])}
+    for I in "HL":
+        out["d_" + I] = np.asarray(z["d_" + I])[rows].astype(complex)
+        key = "sig2_" + I if "sig2_" + I in z else "sig2"
+        out["sig2_" + I] = np.asarray(z[key], float)
+    return out
+
+
+# ----------------------------------------------------------------------------- filter
+
+def trajectories(W, d, sig2, lo, n_time, precision="fp64"):
+    """exmarg/search/bank.py:56-78: z_I = FFT(pad(W conj(d_I) / sig2_I)), ln|z| and arg z.
+
+    W (n_template, n_freq) complex; returns dict lqH, phH, lqL, phL (n_template, n_time),
+    float64 for 'fp64', float32 (complex64 FFT) for 'ref'."""
+    out = {}
+    for I in "HL":
+        if precision == "ref":
+            w = np.ascontiguousarray(np.conj(d[I]) / sig2[I], np.complex64)
+            pad = np.zeros((W.shape[0], n_time), np.complex64)
+            pad[:, lo:lo + W.shape[1]] = np.asarray(W, np.complex64) * w[None, :]
+            z = np.fft.fft(pad, axis=-1)
+            lq = 0.5 * np.log(np.maximum(z.real ** 2 + z.imag ** 2, 1e-38))
+            ph = np.arctan2(z.imag, z.real)
+        else:
+            w = np.conj(d[I]) / sig2[I]
+            pad = np.zeros((W.shape[0], n_time), np.complex128)
+            pad[:, lo:lo + W.shape[1]] = np.asarray(W, np.complex128) * w[None, :]
+            z = np.fft.fft(pad, axis=-1)
+            lq = 0.5 * np.log(np.maximum(z.real ** 2 + z.imag ** 2, 1e-38))
+            ph = np.arctan2(z.imag, z.real)
+        out["lq" + I], out["ph" + I] = lq, ph
+    return out
+
+
+# ----------------------------------------------------------------------------- time selection
+
+def select_times(traj, tau_idx, n_loud, n_random, seed):
+    """exmarg/search/gather.py:374-420: the n_loud loudest times by |z_L|^2 + max_tau |z_H(t+tau)|^2,
+    plus n_random host-RNG draws from the rest with log weight ln((n_time - n_loud) / n_random);
+    returns (sel int32, lw float32), (n_template, n_loud + n_random), sorted by time."""
+    K, S = int(n_loud), int(n_random)
+    lqH, lqL = traj["lqH"], traj["lqL"]
+    nm, nt = lqH.shape
+    lags = np.asarray(tau_idx).ravel().astype(int)
+    lo, hi = int(lags.min()), int(lags.max())
+    if not np.array_equal(np.sort(lags), np.arange(lo, hi + 1)):
+        raise ValueError("lags are not contiguous")
+    pick = np.random.default_rng(seed).integers(0, nt - K, size=(nm, S))
+    # the sliding maximum over lags lo..hi (a direct window maximum; ln|z| is monotone in |z|^2)
+    mx = np.full_like(lqH, -np.inf)
+    for tau in range(lo, hi + 1):
+        mx = np.maximum(mx, np.roll(lqH, -tau, axis=1))
+    score = np.exp(2.0 * lqL) + np.exp(2.0 * mx)
+    sel = np.empty((nm, K + S), np.int64)
+    lw = np.zeros((nm, K + S), np.float32)
+    lw[:, K:] = np.log((nt - K) / S)
+    for m in range(nm):
+        top = np.argpartition(-score[m], K)[:K]
+        rest = np.ones(nt, bool)
+        rest[top] = False
+        rest = np.nonzero(rest)[0]
+        sel[m] = np.concatenate([top, rest[pick[m]]])
+    order = np.argsort(sel, axis=1, kind="stable")
+    return (np.take_along_axis(sel, order, axis=1).astype(np.int32),
+            np.take_along_axis(lw, order, axis=1))
+
+
+# ----------------------------------------------------------------------------- gather
+
+def gather(traj, tables, mass_ids, lna, tab_ids, beta, delta, tau_idx, times=None):
+    """exmarg/search/gather.py:114-140 (gather_cpu contract): (NS, nsel) float64 ln Lambda.
+    float32 trajectories get the reference's float32 phase difference (gather.py:54)."""
+    lib = _lib()
+    phase_f32 = int(np.asarray(traj["phH"]).dtype == np.float32)
+    lqH, phH, lqL, phL = (np.ascontiguousarray(traj[k], np.float64) for k in ("lqH", "phH", "lqL", "phL"))
+    nm, nt = lqH.shape
+    ids = np.ascontiguousarray(mass_ids, np.int64)
+    tab = np.ascontiguousarray(tab_ids, np.int64)
+    lna = np.ascontiguousarray(lna, np.float64)
+    nsel, ns = tab.shape
+    T = [np.ascontiguousarray(t, np.float32) for t in tables]
+    ptrs = (ctypes.c_void_p * len(T))(*[t.ctypes.data for t in T])
+    ntau, nphif, nb, nd = T[0].shape
+    tau = np.ascontiguousarray(tau_idx, np.int64).ravel()
+    if times is not None:
+        sel = np.ascontiguousarray(times[0], np.int32)
+        lw = np.ascontiguousarray(times[1], np.float32)
+        nwalk, psel, plw = sel.shape[1], sel.ctypes.data, lw.ctypes.data
+    else:
+        nwalk, psel, plw = 0, None, None
+    out = np.empty((ns, nsel), np.float64)
+    rc = lib.oracle_gather(nt, lqH.ctypes.data, phH.ctypes.data, lqL.ctypes.data, phL.ctypes.data,
+                           nsel, ns, ids.ctypes.data, tab.ctypes.data, lna.ctypes.data,
+                           ntau, tau.ctypes.data, ptrs, nphif, nb, nd,
+                           float(beta[0]), float(beta[1] - beta[0]), float(delta[0]), float(delta[1] - delta[0]),
+                           nwalk, psel, plw, phase_f32, out.ctypes.data)
+    if rc:
+        raise MemoryError("oracle gather: allocation failed")
+    return out
+
+
+# ----------------------------------------------------------------------------- node geometry, priors
+
+def node_geometry(s, alpha_lo, alpha_hi, u, ymin):
+    """exmarg/search/pe.py:58-84: valid (node, template) pairs, ln a, y, boundary node and its ln a"""
+    nn, nm = s.size, u.size
+    valid = np.zeros((nn, nm), bool)
+    lna = np.zeros((nn, nm))
+    y = np.zeros((nn + 1, nm))
+    bnode = np.full(nm, -1)
+    blna = np.zeros(nm)
+    for k in range(nn):
+        alo = min(alpha_lo[k], ymin * ymin)
+        a = s[k] / u
+        o = (np.sqrt(a) >= ymin) & (a > alo) & (a < alpha_hi[k])
+        valid[k] = o
+        lna[k][o] = np.log(a[o])
+        y[k] = np.where(o, np.sqrt(a), 0.0)
+        s_prev = s[k - 1] if k > 0 else 0.0
+        low = o & (s_prev / u <= alo)
+        a_b = float(alo) * (1.0 + 1e-9)
+        bnode[low] = k
+        blna[low] = np.log(a_b)
+        y[nn][low] = np.sqrt(a_b)
+    return valid, lna, y, bnode, blna
+
+
+def distance_weights(y, prior, ymin, density=None):
+    """exmarg/search/pe.py:260-286: ln of the weights that integrate the distance prior against
+    a likelihood ratio linear in ln y between the points y (ascending).  prior 'volume' is exact;
+    'madau-dickinson' uses the trapezoid rule on 401 points per interval over density (lny, p_lny)."""
+    x = np.log(y)
+    w = np.zeros_like(x)
+    for i in range(x.size - 1):
+        a, b = x[i], x[i + 1]
+        h = b - a
+        if prior == "volume":
+            c, k = 3.0 * ymin ** 3, 3.0
+            ea, eb = np.exp(-k * a), np.exp(-k * b)
+            I0 = (ea - eb) / k
+            I1 = (a * ea - b * eb) / k + (ea - eb) / k ** 2
+            w[i] += c * (b * I0 - I1) / h
+            w[i + 1] += c * (I1 - a * I0) / h
+        else:
+            t = np.linspace(a, b, 401)
+            f = np.interp(t, density[0], density[1], left=0.0, right=0.0)
+            w[i] += np.trapezoid(f * (b - t) / h, t)
+            w[i + 1] += np.trapezoid(f * (t - a) / h, t)
+    with np.errstate(divide="ignore"):
+        return np.log(w)
+
+
+def ln_weights(yN, prior, ymin, density=None):
+    """exmarg/search/pe.py:321-327: lnW (n_node + 1, n_template), -inf where a template has no point"""
+    lnW = np.full(yN.shape, -np.inf)
+    for m in range(yN.shape[1]):
+        pts = np.nonzero(yN[:, m] > 0)[0]
+        if pts.size < 2:
+            raise ValueError("template %d reaches fewer than two store nodes" % m)
+        order = pts[np.argsort(yN[pts, m])]
+        lnW[order, m] = distance_weights(yN[order, m], prior, ymin, density)
+    return lnW
+
+
+def cell_weights(M, q, chi):
+    """exmarg/search/pe.py:338-343: normalised product of the spacings of the distinct values per axis"""
+    cell = np.ones(M.size)
+    for ax in (M, q, chi):
+        vals = np.unique(ax)
+        if vals.size > 1:
+            cell *= np.gradient(vals)[np.searchsorted(vals, ax)]
+    return cell / cell.sum()
+
+
+def log_mean(lam, w):
+    """exmarg/search/pe.py:135-142"""
+    fin = np.isfinite(lam) & (w > 0)
+    if not fin.any():
+        return -np.inf
+    mx = np.where(fin, lam, -np.inf).max()
+    return float(mx + np.log(np.sum(np.where(fin, w * np.exp(np.where(fin, lam, mx) - mx), 0.0))))
+
+
+# ----------------------------------------------------------------------------- pe_intrinsic
+
+def node_values(traj, store, geometry, groups, times):
+    """exmarg/search/pe.py:168-200 for one segment: (n_node + 1, n_template), row n_node the boundary"""
+    valid, lna, _, bnode, blna = geometry
+    nn = store.s.size
+    nm = valid.shape[1]
+    lamN = np.full((nn + 1, nm), -np.inf)
+    for ks in groups:
+        k0 = ks[0]
+        tab = [store.tables[k] for k in ks]
+        beta, delta = store.beta[k0], store.delta[k0]
+        ok = valid[ks]
+        ids = np.nonzero(ok.any(axis=0))[0]
+        lnaM = np.where(ok[:, ids], lna[ks][:, ids], 0.0).T
+        tid = np.tile(np.arange(len(ks)), (ids.size, 1))
+        bids = np.nonzero((bnode >= k0) & (bnode <= ks[-1]))[0]
+        if ids.size:
+            val = gather(traj, tab, ids, lnaM, tid, beta, delta, store.tau_idx, times)
+            for i, k in enumerate(ks):
+                keep = ok[i][ids]
+                lamN[k, ids[keep]] = val[i][keep]
+        if bids.size:
+            val = gather(traj, tab, bids, blna[bids][:, None], (bnode[bids] - k0)[:, None], beta, delta,
+                         store.tau_idx, times)
+            lamN[nn, bids] = val[0]
+    return lamN
+
+
+def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0.1267, nodes_per_launch=6,
+                 n_loud=1024, n_random=1024, seed=0, precision="fp64", density=None, times=None,
+                 return_parts=False):
+    """exmarg/search/pe.py:289-346 for the segments of seg (read_segments output).
+
+    W (n_template, n_freq) complex template factors, u (n_template,) their powers.
+    times: optional list (one per segment) of (sel, lw) to use instead of select_times
+    (so that a numerical comparison is made on the same visited times).
+    returns dict ln_lambda (n_seg, n_template), ln_b (n_seg,) [, parts]"""
+    geometry = node_geometry(store.s, store.alpha_lo, store.alpha_hi, u, ymin)
+    yN = geometry[2]
+    nn = store.s.size
+    groups = [list(range(g, min(g + nodes_per_launch, nn))) for g in range(0, nn, nodes_per_launch)]
+    lnW = ln_weights(yN, prior, ymin, density)
+    nseg = seg["rows"].size
+    out = np.full((nseg, u.size), -np.inf)
+    parts = []
+    for e in range(nseg):
+        traj = trajectories(W, {I: seg["d_" + I][e] for I in "HL"}, {I: seg["sig2_" + I] for I in "HL"},
+                            lo, n_time, precision)
+        if times is not None:
+            tm = times[e]
+        elif n_loud > 0:
+            tm = select_times(traj, store.tau_idx, n_loud, n_random, seed + int(seg["rows"][e]))
+        else:
+            tm = None
+        lamN = node_values(traj, store, geometry, groups, tm)
+        v = lnW + lamN
+        mx = v.max(axis=0)
+        out[e] = mx + np.log(np.exp(v - mx[None, :]).sum(axis=0))
+        if return_parts:
+            parts.append(dict(lamN=lamN, times=tm, traj=traj))
+    w = cell_weights(M, q, chi)
+    ln_b = np.array([log_mean(L, w) for L in out])
+    res = dict(ln_lambda=out, ln_b=ln_b, lnW=lnW)
+    if return_parts:
+        res["parts"] = parts
+    return res
