@@ -1,0 +1,219 @@
+"""ctypes binding of libexmarg_b200.so (include/exmarg_b200.h) and the device context.
+
+The library is built in-tree (exmarg_b200/build.py).  There is no CPU fallback:
+if the shared library is missing or no CUDA device can be opened, every call
+raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexmarg_b200.so")
+
+EXM_OK, EXM_ERR_ARG, EXM_ERR_OOM, EXM_ERR_CUDA, EXM_ERR_TIMEOUT, EXM_ERR_STATE = range(6)
+DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
+PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
+
+# every symbol include/exmarg_b200.h declares
+SYMBOLS = ("exm_version", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+           "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
+           "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
+           "exm_gather", "exm_node_values")
+
+_lib = None
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def load():
+    """the shared library with argument types set (raises if it is not built)"""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libexmarg_b200.so is not built: run python -m exmarg_b200.build (or __graft_entry__.build())")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I, D, Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+    sig = {
+        "exm_version": ([], I),
+        "exm_ctx_create": ([I, Z, ctypes.POINTER(P)], I),
+        "exm_ctx_destroy": ([P], None),
+        "exm_last_error": ([P], ctypes.c_char_p),
+        "exm_ctx_bytes": ([P], Z),
+        "exm_store_init": ([P, I, I, I, I, I, I, P, D, D, D, D], I),
+        "exm_store_set_node": ([P, I, D, D, D, P], I),
+        "exm_store_generate_node": ([P, I, D, D, D, P, P, P, ctypes.c_float, ctypes.c_uint32], I),
+        "exm_store_get_node": ([P, I, P], I),
+        "exm_bank_set": ([P, I, I, I, I, P, P, P, P, P], I),
+        "exm_pe_prepare": ([P, D, I, P, P, I], I),
+        "exm_pe_intrinsic": ([P, I, P, P, P, P, P, I, I, P, P], I),
+        "exm_filter": ([P, P, P, P, P, P], I),
+        "exm_set_trajectories": ([P, P], I),
+        "exm_select_times": ([P, ctypes.c_int64, I, I, P, P], I),
+        "exm_set_times": ([P, I, P, P], I),
+        "exm_gather": ([P, I, I, P, P, P, P], I),
+        "exm_node_values": ([P, P], I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _raise(code, msg):
+    if code == EXM_ERR_ARG:
+        raise ValueError(msg)
+    if code == EXM_ERR_OOM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)
+
+
+class Context:
+    """one device context of libexmarg_b200 (tables, bank, workspaces, one stream)"""
+
+    def __init__(self, device=0, hbm_budget=0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.exm_ctx_create(int(device), int(hbm_budget), ctypes.byref(h))
+        if rc != EXM_OK:
+            _raise(rc, "cannot open CUDA device %d for libexmarg_b200 (status %d)" % (device, rc))
+        self.h = h
+        self.device = device
+        self.store_token = None
+        self.bank_token = None
+        self.prep_token = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.exm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != EXM_OK:
+            _raise(rc, self.lib.exm_last_error(self.h).decode())
+
+    @property
+    def bytes(self):
+        return int(self.lib.exm_ctx_bytes(self.h))
+
+    # store ------------------------------------------------------------
+    def store_init(self, n_nodes, shape, tau_idx, beta0, dbeta, delta0, ddelta, dtype=DTYPE_F32):
+        ntau, nphif, nb, nd = shape
+        tau = np.ascontiguousarray(tau_idx, np.int64)
+        self._check(self.lib.exm_store_init(self.h, n_nodes, ntau, nphif, nb, nd, dtype, _p(tau), beta0, dbeta,
+                                            delta0, ddelta))
+        self.store_token = self.prep_token = None
+
+    def store_set_node(self, k, s, alpha_lo, alpha_hi, T):
+        T = np.ascontiguousarray(T, np.float32)
+        self._check(self.lib.exm_store_set_node(self.h, k, s, alpha_lo, alpha_hi, _p(T)))
+
+    def store_generate_node(self, k, s, alpha_lo, alpha_hi, M, P, Q, S, seed):
+        M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))
+        self._check(self.lib.exm_store_generate_node(self.h, k, s, alpha_lo, alpha_hi, _p(M), _p(P), _p(Q),
+                                                     ctypes.c_float(S), ctypes.c_uint32(seed)))
+
+    def store_get_node(self, k, shape):
+        out = np.empty(shape, np.float32)
+        self._check(self.lib.exm_store_get_node(self.h, k, _p(out)))
+        return out
+
+    # bank ---------------------------------------------------------------
+    def bank_set(self, W, lo, n_time, u, M, q, chi):
+        W = np.ascontiguousarray(W, np.complex64)
+        u, M, q, chi = (np.ascontiguousarray(x, np.float64) for x in (u, M, q, chi))
+        nm, nf = W.shape
+        self._check(self.lib.exm_bank_set(self.h, nm, nf, int(lo), int(n_time), _p(W), _p(u), _p(M), _p(q), _p(chi)))
+        self.nm, self.nfreq, self.n_time = nm, nf, int(n_time)
+        self.prep_token = None
+
+    def prepare(self, ymin, prior, density=None):
+        if prior == PRIOR_TABULATED:
+            lny = np.ascontiguousarray(density[0], np.float64)
+            p = np.ascontiguousarray(density[1], np.float64)
+            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), prior, _p(lny), _p(p), lny.size))
+        else:
+            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), PRIOR_VOLUME, None, None, 0))
+
+    # analysis -------------------------------------------------------------
+    def pe_intrinsic(self, d_H, d_L, sig2_H, sig2_L, seeds, n_loud, n_random):
+        d_H = np.ascontiguousarray(d_H, np.complex128)
+        d_L = np.ascontiguousarray(d_L, np.complex128)
+        sig2_H = np.ascontiguousarray(sig2_H, np.float64)
+        sig2_L = np.ascontiguousarray(sig2_L, np.float64)
+        n = d_H.shape[0]
+        if d_H.shape[1] != self.nfreq or d_L.shape != d_H.shape or sig2_H.size != self.nfreq:
+            raise ValueError("segment frequency bins (%d) do not match the bank (%d)" % (d_H.shape[1], self.nfreq))
+        seeds = np.ascontiguousarray(seeds, np.int64)
+        lnl = np.empty((n, self.nm), np.float64)
+        lnb = np.empty(n, np.float64)
+        self._check(self.lib.exm_pe_intrinsic(self.h, n, _p(d_H), _p(d_L), _p(sig2_H), _p(sig2_L), _p(seeds),
+                                              int(n_loud), int(n_random), _p(lnl), _p(lnb)))
+        return lnl, lnb
+
+    def filter(self, d_H, d_L, sig2_H, sig2_L, want=True):
+        d_H = np.ascontiguousarray(d_H, np.complex128)
+        d_L = np.ascontiguousarray(d_L, np.complex128)
+        sig2_H = np.ascontiguousarray(sig2_H, np.float64)
+        sig2_L = np.ascontiguousarray(sig2_L, np.float64)
+        out = np.empty((4, self.nm, self.n_time), np.float32) if want else None
+        self._check(self.lib.exm_filter(self.h, _p(d_H), _p(d_L), _p(sig2_H), _p(sig2_L), _p(out)))
+        if out is None:
+            return None
+        return dict(lqH=out[0], phH=out[1], lqL=out[2], phL=out[3])
+
+    def set_trajectories(self, traj):
+        out = np.ascontiguousarray(np.stack([traj["lqH"], traj["phH"], traj["lqL"], traj["phL"]]), np.float32)
+        self._check(self.lib.exm_set_trajectories(self.h, _p(out)))
+
+    def select_times(self, seed, n_loud, n_random):
+        nw = n_loud + n_random
+        sel = np.empty((self.nm, nw), np.int32)
+        lw = np.empty((self.nm, nw), np.float32)
+        self._check(self.lib.exm_select_times(self.h, int(seed), int(n_loud), int(n_random), _p(sel), _p(lw)))
+        return sel, lw
+
+    def set_times(self, times):
+        if times is None:
+            self._check(self.lib.exm_set_times(self.h, 0, None, None))
+            return
+        sel = np.ascontiguousarray(times[0], np.int32)
+        lw = np.ascontiguousarray(times[1], np.float32)
+        self._check(self.lib.exm_set_times(self.h, sel.shape[1], _p(sel), _p(lw)))
+
+    def gather(self, mass_ids, lna, tab_ids):
+        ids = np.ascontiguousarray(mass_ids, np.int64)
+        lna = np.ascontiguousarray(lna, np.float64)
+        tab = np.ascontiguousarray(tab_ids, np.int64)
+        nsel, ns = tab.shape
+        out = np.empty((ns, nsel), np.float64)
+        self._check(self.lib.exm_gather(self.h, nsel, ns, _p(ids), _p(lna), _p(tab), _p(out)))
+        return out
+
+    def node_values(self, n_nodes):
+        out = np.empty((n_nodes + 1, self.nm), np.float64)
+        self._check(self.lib.exm_node_values(self.h, _p(out)))
+        return out
+
+
+_contexts = {}
+
+
+def context(device=0):
+    """the process-wide context of a device (created on first use)"""
+    if device not in _contexts:
+        _contexts[device] = Context(device)
+    return _contexts[device]

@@ -1,0 +1,776 @@
+// The C ABI (include/exmarg_b200.h): context, store, bank, the prepared geometry and
+// the pe_intrinsic pipeline (filter -> select_times -> taps -> plane gather ->
+// node / distance log-sum-exp -> ln B), plus the stage entry points.
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pcg64.cuh"
+
+void exm_make_tmap(exm_ctx *ctx);
+void exm_store_generate(exm_ctx *ctx, int k, const float *M, const float *P, const float *Q, float S, uint32_t seed);
+void exm_run_node_values(exm_ctx *ctx, exm_slot &sl, double *d_lamN);
+void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,
+                                const double *d_p, int n_dens);
+void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S);
+void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
+
+// ------------------------------------------------------------------ memory
+
+void exm_alloc(exm_ctx *ctx, dbuf &b, size_t bytes)
+{
+    if (bytes == 0) bytes = 256;
+    if (ctx->used + bytes > ctx->budget)
+        EXM_THROW(EXM_ERR_OOM, "device memory budget exceeded: need " + std::to_string(bytes) + " more bytes, " +
+                                   std::to_string(ctx->budget - ctx->used) + " left of " +
+                                   std::to_string(ctx->budget));
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        EXM_THROW(EXM_ERR_OOM, std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+    }
+    b.p = p;
+    b.bytes = bytes;
+    ctx->used += bytes;
+}
+
+void exm_free(exm_ctx *ctx, dbuf &b)
+{
+    if (b.p) {
+        cudaFree(b.p);
+        ctx->used -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+void exm_ensure(exm_ctx *ctx, dbuf &b, size_t bytes)
+{
+    if (b.p && b.bytes >= bytes) return;
+    exm_free(ctx, b);
+    exm_alloc(ctx, b, bytes);
+}
+
+static void free_slot(exm_ctx *ctx, exm_slot &s)
+{
+    dbuf *all[] = {&s.traj, &s.keys, &s.picks, &s.rej, &s.sel, &s.hist, &s.win, &s.cnt,
+                   &s.desc, &s.tside, &s.part, &s.lnl, &s.lnb, &s.dev_err, &s.din};
+    for (dbuf *b : all) exm_free(ctx, *b);
+    if (s.hostin.p) cudaFreeHost(s.hostin.p);
+    s.hostin.p = nullptr;
+    s.hostin.bytes = 0;
+}
+
+void exm_fft_plan(exm_ctx *ctx, int batch)
+{
+    if (ctx->plan && ctx->plan_batch == batch && ctx->plan_n == ctx->nt) return;
+    if (ctx->plan) cufftDestroy(ctx->plan);
+    ctx->plan = 0;
+    EXM_CUFFT(cufftCreate(&ctx->plan));
+    EXM_CUFFT(cufftSetAutoAllocation(ctx->plan, 0));
+    long long n = ctx->nt;
+    size_t ws = 0;
+    EXM_CUFFT(cufftMakePlanMany64(ctx->plan, 1, &n, nullptr, 1, n, nullptr, 1, n, CUFFT_C2C, batch, &ws));
+    exm_ensure(ctx, ctx->fftwork, ws);
+    EXM_CUFFT(cufftSetWorkArea(ctx->plan, ctx->fftwork.p));
+    EXM_CUFFT(cufftSetStream(ctx->plan, ctx->stream));
+    ctx->plan_batch = batch;
+    ctx->plan_n = ctx->nt;
+}
+
+// ------------------------------------------------------------------ api plumbing
+
+#define API_BEGIN(ctx)                                                                                             \
+    if (!(ctx)) return EXM_ERR_ARG;                                                                                \
+    try {
+#define API_END(ctx)                                                                                               \
+    }                                                                                                              \
+    catch (const exm_error &e)                                                                                     \
+    {                                                                                                              \
+        (ctx)->err = e.msg;                                                                                        \
+        return e.code;                                                                                             \
+    }                                                                                                              \
+    catch (const std::exception &e)                                                                                \
+    {                                                                                                              \
+        (ctx)->err = e.what();                                                                                     \
+        return EXM_ERR_CUDA;                                                                                       \
+    }                                                                                                              \
+    return EXM_OK;
+
+#define REQUIRE(cond, code, msg)                                                                                   \
+    do {                                                                                                           \
+        if (!(cond)) EXM_THROW(code, msg);                                                                         \
+    } while (0)
+
+extern "C" int exm_version(void) { return 10000; }
+
+extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
+{
+    if (!out) return EXM_ERR_ARG;
+    *out = nullptr;
+    exm_ctx *ctx = new exm_ctx();
+    try {
+        EXM_CUDA(cudaSetDevice(device));
+        ctx->dev = device;
+        EXM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        cudaDeviceProp pr;
+        EXM_CUDA(cudaGetDeviceProperties(&pr, device));
+        ctx->sm_count = pr.multiProcessorCount;
+        ctx->smem_optin = pr.sharedMemPerBlockOptin;
+        if (pr.major < 10) EXM_THROW(EXM_ERR_CUDA, "libexmarg_b200 is built for sm_100a (B200); device is sm_" +
+                                                       std::to_string(pr.major * 10 + pr.minor));
+        size_t fr = 0, tot = 0;
+        EXM_CUDA(cudaMemGetInfo(&fr, &tot));
+        ctx->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+    } catch (const exm_error &e) {
+        fprintf(stderr, "exm_ctx_create: %s\n", e.msg.c_str());
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return e.code;
+    }
+    *out = ctx;
+    return EXM_OK;
+}
+
+extern "C" void exm_ctx_destroy(exm_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->dev);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->plan) cufftDestroy(ctx->plan);
+    free_slot(ctx, ctx->slot);
+    dbuf *all[] = {&ctx->T, &ctx->d_tau, &ctx->d_W, &ctx->d_bhat_off, &ctx->d_bnode, &ctx->d_cb, &ctx->d_lnW,
+                   &ctx->d_cell, &ctx->d_mlo, &ctx->d_mhi, &ctx->d_order, &ctx->d_cki, &ctx->d_ckd, &ctx->fftwork};
+    for (dbuf *b : all) exm_free(ctx, *b);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char *exm_last_error(const exm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" size_t exm_ctx_bytes(const exm_ctx *ctx) { return ctx ? ctx->used : 0; }
+
+// ------------------------------------------------------------------ store
+
+extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, int nb, int nd, int dtype,
+                              const int64_t *tau_idx, double beta0, double dbeta, double delta0, double ddelta)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(n_nodes >= 1 && n_nodes <= EXM_MAX_NODES, EXM_ERR_ARG, "n_nodes must be 1..64");
+    REQUIRE(ntau >= 1 && tau_idx, EXM_ERR_ARG, "need at least one lag");
+    REQUIRE(nphif == EXM_NPHI / 2 + 1, EXM_ERR_ARG, "tables must hold NPHI/2 + 1 = 49 phase planes");
+    REQUIRE(nb >= 2 && nb <= 4096 && nd >= 2 && nd <= 256, EXM_ERR_ARG, "need 2 <= nb <= 4096 and 2 <= nd <= 256");
+    REQUIRE(dtype == EXM_DTYPE_F32, EXM_ERR_ARG, "this build stores float32 tables");
+    REQUIRE(dbeta > 0 && ddelta > 0, EXM_ERR_ARG, "grid steps must be positive");
+    ctx->store_ok = ctx->prep_ok = false;
+    ctx->tmap_ok = false;
+    ctx->nn = n_nodes;
+    ctx->ntau = ntau;
+    ctx->nphif = nphif;
+    ctx->nb = nb;
+    ctx->nd = nd;
+    ctx->ndp = (nd + 3) & ~3;
+    ctx->dtype = dtype;
+    ctx->beta0 = beta0;
+    ctx->dbeta = dbeta;
+    ctx->delta0 = delta0;
+    ctx->ddelta = ddelta;
+    ctx->tau.assign(tau_idx, tau_idx + ntau);
+    ctx->s.assign(n_nodes, 0.0);
+    ctx->alo.assign(n_nodes, 0.0);
+    ctx->ahi.assign(n_nodes, 0.0);
+    ctx->node_set.assign(n_nodes, 0);
+    ctx->tstride = (size_t)ntau * nphif * nb * ctx->ndp;
+    exm_free(ctx, ctx->T);
+    exm_alloc(ctx, ctx->T, ctx->tstride * n_nodes * sizeof(float));
+    EXM_CUDA(cudaMemsetAsync(ctx->T.p, 0, ctx->T.bytes, ctx->stream));
+    std::vector<int> t32(ntau);
+    for (int r = 0; r < ntau; ++r) t32[r] = (int)tau_idx[r];
+    exm_ensure(ctx, ctx->d_tau, sizeof(int) * ntau);
+    EXM_CUDA(cudaMemcpy(ctx->d_tau.p, t32.data(), sizeof(int) * ntau, cudaMemcpyHostToDevice));
+    exm_make_tmap(ctx);
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    API_END(ctx)
+}
+
+static void set_node_meta(exm_ctx *ctx, int k, double s, double alo, double ahi)
+{
+    REQUIRE(ctx->T.p, EXM_ERR_STATE, "exm_store_init first");
+    REQUIRE(k >= 0 && k < ctx->nn, EXM_ERR_ARG, "node index out of range");
+    REQUIRE(s > 0 && alo > 0 && ahi > alo, EXM_ERR_ARG, "node needs s > 0 and 0 < alpha_lo < alpha_hi");
+    if (k > 0 && ctx->node_set[k - 1]) REQUIRE(s > ctx->s[k - 1], EXM_ERR_ARG, "nodes must be added with s ascending");
+    ctx->s[k] = s;
+    ctx->alo[k] = alo;
+    ctx->ahi[k] = ahi;
+    ctx->node_set[k] = 1;
+    ctx->prep_ok = false;
+    ctx->store_ok = std::all_of(ctx->node_set.begin(), ctx->node_set.end(), [](char c) { return c != 0; });
+}
+
+extern "C" int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *T)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(T, EXM_ERR_ARG, "null table");
+    set_node_meta(ctx, k, s, alpha_lo, alpha_hi);
+    float *dst = (float *)ctx->T.p + (size_t)k * ctx->tstride;
+    const size_t rows = (size_t)ctx->ntau * ctx->nphif * ctx->nb;
+    EXM_CUDA(cudaMemcpy2DAsync(dst, ctx->ndp * sizeof(float), T, ctx->nd * sizeof(float), ctx->nd * sizeof(float),
+                               rows, cudaMemcpyHostToDevice, ctx->stream));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    API_END(ctx)
+}
+
+extern "C" int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *M,
+                                       const float *P, const float *Q, float S, uint32_t seed)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(M && P && Q, EXM_ERR_ARG, "null generator factors");
+    set_node_meta(ctx, k, s, alpha_lo, alpha_hi);
+    exm_store_generate(ctx, k, M, P, Q, S, seed);
+    API_END(ctx)
+}
+
+extern "C" int exm_store_get_node(exm_ctx *ctx, int k, float *T_out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->T.p && k >= 0 && k < ctx->nn && T_out, EXM_ERR_ARG, "bad node or output");
+    const float *src = (const float *)ctx->T.p + (size_t)k * ctx->tstride;
+    const size_t rows = (size_t)ctx->ntau * ctx->nphif * ctx->nb;
+    EXM_CUDA(cudaMemcpy2DAsync(T_out, ctx->nd * sizeof(float), src, ctx->ndp * sizeof(float), ctx->nd * sizeof(float),
+                               rows, cudaMemcpyDeviceToHost, ctx->stream));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    API_END(ctx)
+}
+
+// ------------------------------------------------------------------ bank
+
+extern "C" int exm_bank_set(exm_ctx *ctx, int nm, int nfreq, int lo, int n_time, const float *W, const double *u,
+                            const double *M, const double *q, const double *chi)
+{
+    API_BEGIN(ctx)
+    REQUIRE(nm >= 1 && nfreq >= 1 && lo >= 0 && n_time >= 2 && lo + nfreq <= n_time, EXM_ERR_ARG,
+            "bank needs nm >= 1 and lo + nfreq <= n_time");
+    REQUIRE(W && u && M && q && chi, EXM_ERR_ARG, "null bank array");
+    ctx->nm = nm;
+    ctx->nfreq = nfreq;
+    ctx->lo = lo;
+    ctx->nt = n_time;
+    ctx->W.assign(W, W + (size_t)2 * nm * nfreq);
+    ctx->u.assign(u, u + nm);
+    ctx->M.assign(M, M + nm);
+    ctx->q.assign(q, q + nm);
+    ctx->chi.assign(chi, chi + nm);
+    for (int m = 0; m < nm; ++m) REQUIRE(u[m] > 0, EXM_ERR_ARG, "template powers u must be positive");
+    ctx->bank_ok = true;
+    ctx->prep_ok = false;
+    ctx->traj_ok = ctx->times_ok = false;
+    API_END(ctx)
+}
+
+// ------------------------------------------------------------------ prepare: geometry, weights, cell weights
+
+static std::vector<double> cell_weights(const exm_ctx *ctx)
+{
+    const int nm = ctx->nm;
+    std::vector<double> cell(nm, 1.0);
+    const std::vector<double> *axes[3] = {&ctx->M, &ctx->q, &ctx->chi};
+    for (const auto *ax : axes) {
+        std::vector<double> vals(*ax);
+        std::sort(vals.begin(), vals.end());
+        vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+        const int n = (int)vals.size();
+        if (n <= 1) continue;
+        std::vector<double> g(n);
+        g[0] = vals[1] - vals[0];
+        g[n - 1] = vals[n - 1] - vals[n - 2];
+        for (int i = 1; i < n - 1; ++i) g[i] = (vals[i + 1] - vals[i - 1]) / 2.0;
+        for (int m = 0; m < nm; ++m) {
+            const int j = (int)(std::lower_bound(vals.begin(), vals.end(), (*ax)[m]) - vals.begin());
+            cell[m] *= g[j];
+        }
+    }
+    double tot = 0.0;
+    for (double c : cell) tot += c;
+    for (double &c : cell) c /= tot;
+    return cell;
+}
+
+template <typename T>
+static void upload(exm_ctx *ctx, dbuf &b, const std::vector<T> &v)
+{
+    exm_ensure(ctx, b, sizeof(T) * std::max<size_t>(v.size(), 1));
+    if (!v.empty()) EXM_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+}
+
+extern "C" int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double *lny, const double *p_lny, int n_dens)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->store_ok, EXM_ERR_STATE, "store is not complete (exm_store_init + every node)");
+    REQUIRE(ctx->bank_ok, EXM_ERR_STATE, "no bank (exm_bank_set)");
+    REQUIRE(prior == EXM_PRIOR_VOLUME || (prior == EXM_PRIOR_TABULATED && lny && p_lny && n_dens >= 2), EXM_ERR_ARG,
+            "the distance prior is 'volume' or a tabulated density");
+    const int nn = ctx->nn, nm = ctx->nm;
+    // node geometry, exmarg/search/pe.py:58-84, on the original template order
+    std::vector<char> valid((size_t)nn * nm, 0);
+    std::vector<double> y((size_t)(nn + 1) * nm, 0.0);
+    std::vector<int> bnode(nm, -1);
+    std::vector<double> blna(nm, 0.0);
+    for (int k = 0; k < nn; ++k) {
+        const double alo = std::min(ctx->alo[k], ymin * ymin);
+        const double s_prev = k > 0 ? ctx->s[k - 1] : 0.0;
+        const double a_b = alo * (1.0 + 1e-9);
+        for (int m = 0; m < nm; ++m) {
+            const double a = ctx->s[k] / ctx->u[m];
+            const bool o = (std::sqrt(a) >= ymin) && (a > alo) && (a < ctx->ahi[k]);
+            valid[(size_t)k * nm + m] = o;
+            y[(size_t)k * nm + m] = o ? std::sqrt(a) : 0.0;
+            if (o && (s_prev / ctx->u[m] <= alo)) {
+                bnode[m] = k;
+                blna[m] = std::log(a_b);
+                y[(size_t)nn * nm + m] = std::sqrt(a_b);
+            }
+        }
+    }
+    for (int m = 0; m < nm; ++m) {
+        int pts = 0;
+        for (int k = 0; k <= nn; ++k) pts += y[(size_t)k * nm + m] > 0;
+        if (pts < 2) {
+            char buf[160];
+            snprintf(buf, sizeof(buf), "template %d (M %.2f, u %.3f) reaches fewer than two store nodes", m,
+                     ctx->M[m], ctx->u[m]);
+            EXM_THROW(EXM_ERR_ARG, buf);
+        }
+    }
+    // internal order: ascending u, so every node's valid templates form one range
+    std::vector<int> order(nm);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return ctx->u[a] < ctx->u[b]; });
+    ctx->order = order;
+    ctx->mlo.assign(nn, 0);
+    ctx->mhi.assign(nn, 0);
+    for (int k = 0; k < nn; ++k) {
+        int first = -1, last = -1;
+        for (int i = 0; i < nm; ++i)
+            if (valid[(size_t)k * nm + order[i]]) {
+                if (first < 0) first = i;
+                last = i;
+            }
+        if (first < 0) {
+            ctx->mlo[k] = ctx->mhi[k] = 0;
+            continue;
+        }
+        for (int i = first; i <= last; ++i)
+            REQUIRE(valid[(size_t)k * nm + order[i]], EXM_ERR_ARG,
+                    "node validity is not an interval in u (alpha limits vary across nodes)");
+        ctx->mlo[k] = first;
+        ctx->mhi[k] = last + 1;
+    }
+    std::vector<int> bn(nm);
+    std::vector<double> boff(nm), cb(nm, 0.0), yint((size_t)(nn + 1) * nm), cellv = cell_weights(ctx), celli(nm);
+    for (int i = 0; i < nm; ++i) {
+        const int m = order[i];
+        bn[i] = bnode[m];
+        boff[i] = -std::log(ctx->u[m]) / ctx->dbeta;
+        if (bnode[m] >= 0) cb[i] = (blna[m] - ctx->beta0) / ctx->dbeta + std::log(ctx->u[m]) / ctx->dbeta;
+        for (int k = 0; k <= nn; ++k) yint[(size_t)k * nm + i] = y[(size_t)k * nm + m];
+        celli[i] = cellv[m];
+    }
+    ctx->bnode = bn;
+    ctx->ck.assign(nn, 0.0);
+    std::vector<int> cki(EXM_MAX_NODES, 0);
+    std::vector<double> ckd(EXM_MAX_NODES, 0.0);
+    for (int k = 0; k < nn; ++k) {
+        ctx->ck[k] = (std::log(ctx->s[k]) - ctx->beta0) / ctx->dbeta;
+        ckd[k] = ctx->ck[k];
+        cki[k] = (int)std::floor(ctx->ck[k]);
+    }
+    // W in internal order
+    std::vector<float> Wi((size_t)2 * nm * ctx->nfreq);
+    for (int i = 0; i < nm; ++i)
+        memcpy(&Wi[(size_t)2 * i * ctx->nfreq], &ctx->W[(size_t)2 * order[i] * ctx->nfreq],
+               sizeof(float) * 2 * ctx->nfreq);
+    upload(ctx, ctx->d_W, Wi);
+    upload(ctx, ctx->d_bhat_off, boff);
+    upload(ctx, ctx->d_bnode, bn);
+    upload(ctx, ctx->d_cb, cb);
+    upload(ctx, ctx->d_cell, celli);
+    upload(ctx, ctx->d_mlo, ctx->mlo);
+    upload(ctx, ctx->d_mhi, ctx->mhi);
+    upload(ctx, ctx->d_order, order);
+    upload(ctx, ctx->d_cki, cki);
+    upload(ctx, ctx->d_ckd, ckd);
+    // distance-prior weights on the device
+    dbuf dy, dd;
+    upload(ctx, dy, yint);
+    std::vector<double> dens;
+    if (prior == EXM_PRIOR_TABULATED) {
+        dens.assign(lny, lny + n_dens);
+        dens.insert(dens.end(), p_lny, p_lny + n_dens);
+    }
+    upload(ctx, dd, dens);
+    exm_ensure(ctx, ctx->d_lnW, sizeof(double) * (size_t)(nn + 1) * nm);
+    exm_run_distance_weights_y(ctx, (const double *)dy.p, ymin, prior, (const double *)dd.p,
+                               (const double *)dd.p + (dens.empty() ? 0 : n_dens), n_dens);
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    exm_free(ctx, dy);
+    exm_free(ctx, dd);
+    ctx->prep_ok = true;
+    ctx->traj_ok = ctx->times_ok = false;
+    API_END(ctx)
+}
+
+// ------------------------------------------------------------------ the per-segment pipeline
+
+struct RunShape {
+    int K, S, nwalk, use_sel, nmc_max, rc;
+    float lw;
+};
+
+static RunShape run_shape(exm_ctx *ctx, int K, int S)
+{
+    RunShape rs;
+    REQUIRE(K >= 0 && S >= 0, EXM_ERR_ARG, "n_loud and n_random must be >= 0");
+    rs.K = K;
+    rs.S = S;
+    if (K > 0) {
+        REQUIRE(S >= 1, EXM_ERR_ARG, "n_random must be >= 1 when n_loud > 0 (division by zero)");
+        REQUIRE(ctx->nt - K >= 1, EXM_ERR_ARG, "high <= 0: n_loud must be below n_time");
+        std::vector<int64_t> t = ctx->tau;
+        std::sort(t.begin(), t.end());
+        for (size_t i = 1; i < t.size(); ++i) REQUIRE(t[i] == t[i - 1] + 1, EXM_ERR_ARG, "lags are not contiguous");
+        rs.nwalk = K + S;
+        rs.use_sel = 1;
+        rs.lw = (float)std::log((double)(ctx->nt - K) / (double)S);
+    } else {
+        rs.nwalk = ctx->nt;
+        rs.use_sel = 0;
+        rs.lw = 0.f;
+    }
+    rs.nmc_max = std::min(ctx->nm, EXM_MAX_CHUNK);
+    const size_t per_lag = (size_t)rs.nmc_max * rs.nwalk * 20;
+    const size_t cap = (size_t)8 << 30;
+    rs.rc = (int)std::max<size_t>(1, std::min<size_t>((size_t)ctx->ntau, cap / std::max<size_t>(per_lag, 1)));
+    return rs;
+}
+
+static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
+{
+    const size_t nmc = rs.nmc_max, nt = ctx->nt, nf = ctx->nfreq;
+    exm_ensure(ctx, sl.traj, 2 * nmc * nt * sizeof(float2));
+    const size_t n_draws = rs.K > 0 ? (((size_t)ctx->nm * rs.S + EXM_MAX_REJ + 63) / 64) * 64 : 0;
+    exm_ensure(ctx, sl.keys, std::max<size_t>(rs.K > 0 ? nmc * nt : 1, n_draws) * sizeof(uint32_t));
+    exm_ensure(ctx, sl.picks, std::max<size_t>(1, (size_t)ctx->nm * rs.S) * sizeof(int32_t));
+    exm_ensure(ctx, sl.rej, (1 + EXM_MAX_REJ) * sizeof(int));
+    exm_ensure(ctx, sl.sel, std::max<size_t>(1, rs.use_sel ? nmc * rs.nwalk : 1) * sizeof(int32_t));
+    exm_ensure(ctx, sl.hist, (EXM_HB_N + 256) * sizeof(int));
+    exm_ensure(ctx, sl.win, (1 + EXM_MAX_NODES) * sizeof(int));
+    exm_ensure(ctx, sl.cnt, (size_t)rs.rc * EXM_NPAIR * (nmc + 1) * sizeof(int));
+    exm_ensure(ctx, sl.desc, (size_t)rs.rc * nmc * rs.nwalk * sizeof(uint4));
+    exm_ensure(ctx, sl.tside, (size_t)rs.rc * nmc * rs.nwalk * sizeof(int32_t));
+    exm_ensure(ctx, sl.part, (size_t)(ctx->nn + 1) * ctx->ntau * ctx->nm * sizeof(double));
+    exm_ensure(ctx, sl.lnl, (size_t)ctx->nm * sizeof(double));
+    exm_ensure(ctx, sl.lnb, sizeof(double));
+    exm_ensure(ctx, sl.dev_err, sizeof(unsigned));
+    exm_ensure(ctx, sl.din, 6 * nf * sizeof(double) + 2 * nf * sizeof(float2));
+    const size_t hin = 6 * nf * sizeof(double);
+    if (!sl.hostin.p || sl.hostin.bytes < hin) {
+        if (sl.hostin.p) cudaFreeHost(sl.hostin.p);
+        sl.hostin.p = nullptr;
+        EXM_CUDA(cudaMallocHost(&sl.hostin.p, hin));
+        sl.hostin.bytes = hin;
+    }
+}
+
+static void stage_input(exm_ctx *ctx, exm_slot &sl, const double *dH, const double *dL, const double *s2H,
+                        const double *s2L)
+{
+    const size_t nf = ctx->nfreq;
+    double *h = (double *)sl.hostin.p;
+    memcpy(h, dH, 2 * nf * sizeof(double));
+    memcpy(h + 2 * nf, dL, 2 * nf * sizeof(double));
+    memcpy(h + 4 * nf, s2H, nf * sizeof(double));
+    memcpy(h + 5 * nf, s2L, nf * sizeof(double));
+    EXM_CUDA(cudaMemcpyAsync(sl.din.p, h, 6 * nf * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+}
+
+static void check_dev_err(exm_ctx *ctx, exm_slot &sl)
+{
+    unsigned e = 0;
+    EXM_CUDA(cudaMemcpyAsync(&e, sl.dev_err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (e & EXM_DEVERR_TIMEOUT)
+        EXM_THROW(EXM_ERR_TIMEOUT, "a bounded device wait (TMA copy of a table plane) ran out");
+    if (e & EXM_DEVERR_BOUNDS) EXM_THROW(EXM_ERR_CUDA, "a tap descriptor pointed outside its block (internal error)");
+}
+
+// everything of one segment from the staged input to lnl / lnb on the device
+static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs, uint64_t seed)
+{
+    EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
+    if (rs.K > 0) exm_run_pcg(ctx, sl, seed, rs.K, rs.S);
+    for (int m_base = 0; m_base < ctx->nm; m_base += rs.nmc_max) {
+        const int nmc = std::min(rs.nmc_max, ctx->nm - m_base);
+        exm_run_filter(ctx, sl, (const float2 *)ctx->d_W.p + (size_t)m_base * ctx->nfreq, nmc);
+        if (rs.K > 0) exm_run_topk(ctx, sl, nmc, (const int *)ctx->d_order.p + m_base, rs.K, rs.S);
+        ChunkInfo ci{m_base, nmc, rs.nwalk, rs.use_sel, rs.lw};
+        for (int r0 = 0; r0 < ctx->ntau; r0 += rs.rc) {
+            const int rc = std::min(rs.rc, ctx->ntau - r0);
+            exm_run_taps(ctx, sl, ci, r0, rc, r0 == 0);
+            exm_run_gather_planes(ctx, sl, ci, r0, rc);
+        }
+        exm_run_node_lse(ctx, sl, m_base, nmc);
+    }
+    exm_run_lnb(ctx, sl);
+}
+
+extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const double *d_L, const double *sig2_H,
+                                const double *sig2_L, const int64_t *seeds, int n_loud, int n_random,
+                                double *ln_lambda, double *ln_b)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->prep_ok, EXM_ERR_STATE, "exm_pe_prepare first");
+    REQUIRE(n_seg >= 0 && d_H && d_L && sig2_H && sig2_L && ln_lambda && ln_b, EXM_ERR_ARG, "null argument");
+    REQUIRE(n_loud == 0 || seeds, EXM_ERR_ARG, "seeds are needed when n_loud > 0");
+    const RunShape rs = run_shape(ctx, n_loud, n_random);
+    exm_slot &sl = ctx->slot;
+    ensure_slot(ctx, sl, rs);
+    std::vector<double> lnl(ctx->nm);
+    const size_t nf = ctx->nfreq;
+    for (int e = 0; e < n_seg; ++e) {
+        REQUIRE(rs.K == 0 || seeds[e] >= 0, EXM_ERR_ARG, "seed must be non-negative");
+        stage_input(ctx, sl, d_H + (size_t)e * 2 * nf, d_L + (size_t)e * 2 * nf, sig2_H, sig2_L);
+        run_segment(ctx, sl, rs, rs.K > 0 ? (uint64_t)seeds[e] : 0);
+        EXM_CUDA(cudaMemcpyAsync(lnl.data(), sl.lnl.p, sizeof(double) * ctx->nm, cudaMemcpyDeviceToHost, ctx->stream));
+        EXM_CUDA(cudaMemcpyAsync(ln_b + e, sl.lnb.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        check_dev_err(ctx, sl);
+        for (int i = 0; i < ctx->nm; ++i) ln_lambda[(size_t)e * ctx->nm + ctx->order[i]] = lnl[i];
+    }
+    ctx->traj_ok = ctx->times_ok = false;
+    API_END(ctx)
+}
+
+// ------------------------------------------------------------------ stage entry points
+
+static RunShape stage_shape(exm_ctx *ctx, int K, int S)
+{
+    REQUIRE(ctx->prep_ok, EXM_ERR_STATE, "exm_pe_prepare first");
+    REQUIRE(ctx->nm <= EXM_MAX_CHUNK, EXM_ERR_ARG, "stage entry points take banks of at most 8192 templates");
+    return run_shape(ctx, K, S);
+}
+
+extern "C" int exm_filter(exm_ctx *ctx, const double *d_H, const double *d_L, const double *sig2_H,
+                          const double *sig2_L, float *traj_out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    RunShape rs = stage_shape(ctx, 0, 0);
+    exm_slot &sl = ctx->slot;
+    ensure_slot(ctx, sl, rs);
+    stage_input(ctx, sl, d_H, d_L, sig2_H, sig2_L);
+    exm_run_filter(ctx, sl, (const float2 *)ctx->d_W.p, ctx->nm);
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->traj_ok = true;
+    ctx->times_ok = false;
+    ctx->cur_nwalk = ctx->nt;
+    ctx->cur_lw = 0.f;
+    if (traj_out) {
+        const size_t nt = ctx->nt, nm = ctx->nm;
+        std::vector<float2> h(2 * nm * nt);
+        EXM_CUDA(cudaMemcpy(h.data(), sl.traj.p, sizeof(float2) * h.size(), cudaMemcpyDeviceToHost));
+        for (int det = 0; det < 2; ++det)
+            for (size_t i = 0; i < nm; ++i) {
+                const size_t m = ctx->order[i];
+                const float2 *src = &h[(det * nm + i) * nt];
+                float *lq = traj_out + ((size_t)(2 * det) * nm + m) * nt;
+                float *ph = traj_out + ((size_t)(2 * det + 1) * nm + m) * nt;
+                for (size_t t = 0; t < nt; ++t) {
+                    lq[t] = src[t].x;
+                    ph[t] = src[t].y;
+                }
+            }
+    }
+    API_END(ctx)
+}
+
+extern "C" int exm_set_trajectories(exm_ctx *ctx, const float *traj)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(traj, EXM_ERR_ARG, "null trajectories");
+    RunShape rs = stage_shape(ctx, 0, 0);
+    exm_slot &sl = ctx->slot;
+    ensure_slot(ctx, sl, rs);
+    const size_t nt = ctx->nt, nm = ctx->nm;
+    std::vector<float2> h(2 * nm * nt);
+    for (int det = 0; det < 2; ++det)
+        for (size_t i = 0; i < nm; ++i) {
+            const size_t m = ctx->order[i];
+            const float *lq = traj + ((size_t)(2 * det) * nm + m) * nt;
+            const float *ph = traj + ((size_t)(2 * det + 1) * nm + m) * nt;
+            float2 *dst = &h[(det * nm + i) * nt];
+            for (size_t t = 0; t < nt; ++t) dst[t] = make_float2(lq[t], ph[t]);
+        }
+    EXM_CUDA(cudaMemcpy(sl.traj.p, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+    ctx->traj_ok = true;
+    ctx->times_ok = false;
+    ctx->cur_nwalk = ctx->nt;
+    ctx->cur_lw = 0.f;
+    API_END(ctx)
+}
+
+extern "C" int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_random, int32_t *sel_out, float *lw_out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->traj_ok, EXM_ERR_STATE, "no trajectories (exm_filter or exm_set_trajectories first)");
+    REQUIRE(n_loud > 0, EXM_ERR_ARG, "select_times needs n_loud > 0");
+    REQUIRE(seed >= 0, EXM_ERR_ARG, "seed must be non-negative");
+    RunShape rs = stage_shape(ctx, n_loud, n_random);
+    exm_slot &sl = ctx->slot;
+    ensure_slot(ctx, sl, rs);
+    exm_run_pcg(ctx, sl, (uint64_t)seed, rs.K, rs.S);
+    exm_run_topk(ctx, sl, ctx->nm, (const int *)ctx->d_order.p, rs.K, rs.S);
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->times_ok = true;
+    ctx->cur_nwalk = rs.nwalk;
+    ctx->cur_lw = rs.lw;
+    if (sel_out || lw_out) {
+        const size_t nw = rs.nwalk, nm = ctx->nm;
+        std::vector<int32_t> h(nm * nw);
+        EXM_CUDA(cudaMemcpy(h.data(), sl.sel.p, sizeof(int32_t) * h.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < nm; ++i) {
+            const size_t m = ctx->order[i];
+            for (size_t w = 0; w < nw; ++w) {
+                const int32_t v = h[i * nw + w];
+                if (sel_out) sel_out[m * nw + w] = v & 0x7FFFFFFF;
+                if (lw_out) lw_out[m * nw + w] = (v < 0) ? rs.lw : 0.f;
+            }
+        }
+    }
+    API_END(ctx)
+}
+
+extern "C" int exm_set_times(exm_ctx *ctx, int nwalk, const int32_t *sel, const float *lw)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->traj_ok, EXM_ERR_STATE, "no trajectories");
+    REQUIRE(nwalk >= 0, EXM_ERR_ARG, "nwalk must be >= 0");
+    if (nwalk == 0) {
+        ctx->times_ok = false;
+        ctx->cur_nwalk = ctx->nt;
+        ctx->cur_lw = 0.f;
+        return EXM_OK;
+    }
+    REQUIRE(sel && lw, EXM_ERR_ARG, "null times");
+    const size_t nm = ctx->nm;
+    float lwv = 0.f;
+    std::vector<int32_t> h(nm * nwalk);
+    for (size_t i = 0; i < nm; ++i) {
+        const size_t m = ctx->order[i];
+        for (int w = 0; w < nwalk; ++w) {
+            const int32_t t = sel[m * nwalk + w];
+            const float l = lw[m * nwalk + w];
+            REQUIRE(t >= 0 && t < ctx->nt, EXM_ERR_ARG, "time index out of range");
+            if (l != 0.f) {
+                REQUIRE(lwv == 0.f || lwv == l, EXM_ERR_ARG, "every drawn time must carry the same log weight");
+                lwv = l;
+            }
+            h[i * nwalk + w] = t | (l != 0.f ? (int32_t)0x80000000 : 0);
+        }
+    }
+    RunShape rs = stage_shape(ctx, 0, 0);
+    rs.nwalk = nwalk;
+    rs.use_sel = 1;
+    exm_slot &sl = ctx->slot;
+    exm_ensure(ctx, sl.sel, sizeof(int32_t) * h.size());
+    EXM_CUDA(cudaMemcpy(sl.sel.p, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice));
+    ctx->times_ok = true;
+    ctx->cur_nwalk = nwalk;
+    ctx->cur_lw = lwv;
+    API_END(ctx)
+}
+
+extern "C" int exm_gather(exm_ctx *ctx, int nsel, int ns, const int64_t *mass_ids, const double *lna,
+                          const int64_t *tab_ids, double *out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->traj_ok, EXM_ERR_STATE, "no trajectories");
+    REQUIRE(nsel >= 1 && ns >= 1 && mass_ids && lna && tab_ids && out, EXM_ERR_ARG, "bad gather arguments");
+    std::vector<int> rows(nsel), tab((size_t)nsel * ns);
+    std::vector<int> rank(ctx->nm);
+    for (int i = 0; i < ctx->nm; ++i) rank[ctx->order[i]] = i;
+    for (int j = 0; j < nsel; ++j) {
+        REQUIRE(mass_ids[j] >= 0 && mass_ids[j] < ctx->nm, EXM_ERR_ARG, "mass id out of range");
+        rows[j] = rank[mass_ids[j]];
+        for (int n = 0; n < ns; ++n) {
+            const int64_t t = tab_ids[(size_t)j * ns + n];
+            REQUIRE(t >= 0 && t < ctx->nn, EXM_ERR_ARG, "table id out of range");
+            tab[(size_t)j * ns + n] = (int)t;
+        }
+    }
+    exm_slot &sl = ctx->slot;
+    dbuf drows, dtab, dlna, dout;
+    upload(ctx, drows, rows);
+    upload(ctx, dtab, tab);
+    std::vector<double> l(lna, lna + (size_t)nsel * ns);
+    upload(ctx, dlna, l);
+    exm_alloc(ctx, dout, sizeof(double) * (size_t)nsel * ns);
+    exm_ensure(ctx, sl.part, std::max(sl.part.bytes, sizeof(double) * 2 * (size_t)ns * ctx->ntau * nsel));
+    exm_run_gather_simple(ctx, sl, nsel, ns, (const int *)drows.p, (const int *)dtab.p, (const double *)dlna.p,
+                          ctx->times_ok ? ctx->cur_nwalk : ctx->nt, ctx->times_ok ? 1 : 0, ctx->cur_lw,
+                          (double *)dout.p);
+    EXM_CUDA(cudaMemcpyAsync(out, dout.p, sizeof(double) * (size_t)nsel * ns, cudaMemcpyDeviceToHost, ctx->stream));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    exm_free(ctx, drows);
+    exm_free(ctx, dtab);
+    exm_free(ctx, dlna);
+    exm_free(ctx, dout);
+    API_END(ctx)
+}
+
+extern "C" int exm_node_values(exm_ctx *ctx, double *lamN_out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->traj_ok, EXM_ERR_STATE, "no trajectories");
+    REQUIRE(lamN_out, EXM_ERR_ARG, "null output");
+    RunShape rs = stage_shape(ctx, 0, 0);
+    rs.nwalk = ctx->times_ok ? ctx->cur_nwalk : ctx->nt;
+    rs.use_sel = ctx->times_ok ? 1 : 0;
+    rs.lw = ctx->cur_lw;
+    const size_t per_lag = (size_t)ctx->nm * rs.nwalk * 20;
+    rs.rc = (int)std::max<size_t>(1, std::min<size_t>((size_t)ctx->ntau, ((size_t)8 << 30) / per_lag));
+    exm_slot &sl = ctx->slot;
+    exm_ensure(ctx, sl.cnt, (size_t)rs.rc * EXM_NPAIR * (ctx->nm + 1) * sizeof(int));
+    exm_ensure(ctx, sl.desc, (size_t)rs.rc * ctx->nm * rs.nwalk * sizeof(uint4));
+    exm_ensure(ctx, sl.tside, (size_t)rs.rc * ctx->nm * rs.nwalk * sizeof(int32_t));
+    exm_ensure(ctx, sl.part, (size_t)(ctx->nn + 1) * ctx->ntau * ctx->nm * sizeof(double));
+    EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
+    ChunkInfo ci{0, ctx->nm, rs.nwalk, rs.use_sel, rs.lw};
+    for (int r0 = 0; r0 < ctx->ntau; r0 += rs.rc) {
+        const int rc = std::min(rs.rc, ctx->ntau - r0);
+        exm_run_taps(ctx, sl, ci, r0, rc, r0 == 0);
+        exm_run_gather_planes(ctx, sl, ci, r0, rc);
+    }
+    dbuf dl;
+    exm_alloc(ctx, dl, sizeof(double) * (size_t)(ctx->nn + 1) * ctx->nm);
+    exm_run_node_values(ctx, sl, (double *)dl.p);
+    std::vector<double> h((size_t)(ctx->nn + 1) * ctx->nm);
+    EXM_CUDA(cudaMemcpyAsync(h.data(), dl.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    check_dev_err(ctx, sl);
+    exm_free(ctx, dl);
+    for (int k = 0; k <= ctx->nn; ++k)
+        for (int i = 0; i < ctx->nm; ++i) lamN_out[(size_t)k * ctx->nm + ctx->order[i]] = h[(size_t)k * ctx->nm + i];
+    API_END(ctx)
+}

@@ -1,0 +1,135 @@
+// Shared definitions of libexmarg_b200: the context, device-memory accounting,
+// error reporting and the constants of the table geometry.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/exmarg_b200.h"
+
+#define EXM_NPHI 96     // phase bins of the full circle (exmarg/search/gather.py:29)
+#define EXM_NPAIR 48    // plane pairs (p, p+1), p = 0..47, of the 49 stored phase planes
+
+// ------------------------------------------------------------------ errors
+
+struct exm_error {
+    int code;
+    std::string msg;
+};
+
+#define EXM_THROW(code, msg) throw exm_error{(code), (msg)}
+#define EXM_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            throw exm_error{EXM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)};      \
+    } while (0)
+#define EXM_CUFFT(call)                                                                             \
+    do {                                                                                            \
+        cufftResult r_ = (call);                                                                    \
+        if (r_ != CUFFT_SUCCESS)                                                                    \
+            throw exm_error{EXM_ERR_CUDA, std::string(#call) + ": cufft error " + std::to_string((int)r_)}; \
+    } while (0)
+
+// device error word: set by kernels whose bounded waits ran out
+#define EXM_DEVERR_TIMEOUT 1u
+#define EXM_DEVERR_BOUNDS 2u
+
+// ------------------------------------------------------------------ device buffers
+
+struct exm_ctx;
+
+struct dbuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// per-segment workspace of the analysis pipeline
+struct exm_slot {
+    dbuf traj;      // float2 [2][nm][nt]: (ln|z|, arg z) of H then L
+    dbuf keys;      // uint32 [nm][nt]: selection scores as ordered integers
+    dbuf picks;     // int32 [nm][S]: random ranks into the rest
+    dbuf rej;       // int32 [1 + EXM_MAX_REJ]: rejected draw positions
+    dbuf sel;       // int32 [nm][nwalk]: visited time, bit 31 set for a random draw
+    dbuf hist;      // int32 histograms for the staging windows
+    dbuf win;       // int32 window origins
+    dbuf cnt;       // int32 [rc][48][nm+1]: taps per (lag, plane pair, template) -> offsets
+    dbuf desc;      // uint4 [rc][nm*nwalk]: tap descriptors sorted by (plane pair, template)
+    dbuf tside;     // int32 [rc][nm*nwalk]: time index of each descriptor (slow path)
+    dbuf part;      // double [nn+1][ntau][nm]: ln of the per-lag sums
+    dbuf lnl;       // double [nm]
+    dbuf lnb;       // double [1]
+    dbuf dev_err;   // uint32 [1]
+    dbuf hostin;    // pinned host staging (d_H, d_L)
+    dbuf din;       // device copy of d_H, d_L complex128 and sig2
+    int nwalk = 0, rc = 0;
+};
+
+#define EXM_MAX_REJ 4096
+
+struct exm_ctx {
+    int dev = 0;
+    size_t budget = 0, used = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sm_count = 148;
+    size_t smem_optin = 0;
+
+    // store
+    bool store_ok = false;
+    int nn = 0, ntau = 0, nphif = 0, nb = 0, nd = 0, ndp = 0, dtype = 0;
+    double beta0 = 0, dbeta = 0, delta0 = 0, ddelta = 0;
+    std::vector<int64_t> tau;
+    std::vector<double> s, alo, ahi;
+    std::vector<char> node_set;
+    dbuf T;             // [nn][ntau][nphif][nb][ndp]
+    size_t tstride = 0; // elements per node
+    dbuf d_tau;         // int32 [ntau]
+    CUtensorMap tmap;   // 5-D map over T for the plane windows
+    bool tmap_ok = false;
+
+    // bank (original order)
+    bool bank_ok = false;
+    int nm = 0, nfreq = 0, lo = 0, nt = 0;
+    std::vector<float> W;
+    std::vector<double> u, M, q, chi;
+
+    // prepared analysis (internal order: templates sorted by u)
+    bool prep_ok = false;
+    std::vector<int> order;           // internal -> original
+    std::vector<int> mlo, mhi;        // per node: valid internal template range
+    std::vector<int> bnode;           // internal: boundary node or -1
+    dbuf d_W;                         // float2 [nm][nfreq], internal order
+    dbuf d_bhat_off;                  // double [nm]: -ln(u)/dbeta
+    dbuf d_bnode;                     // int32 [nm]
+    dbuf d_cb;                        // double [nm]: boundary offset (ln u + ln a_b - beta0)/dbeta
+    dbuf d_lnW;                       // double [nn+1][nm]
+    dbuf d_cell;                      // double [nm]
+    dbuf d_mlo, d_mhi;                // int32 [nn]
+    dbuf d_order;                     // int32 [nm]
+    std::vector<double> ck;           // (ln s_k - beta0) / dbeta
+    dbuf d_cki;                       // int32 [EXM_MAX_NODES]: floor(ck)
+    dbuf d_ckd;                       // double [EXM_MAX_NODES]: ck
+
+    // cuFFT
+    cufftHandle plan = 0;
+    int plan_batch = 0, plan_n = 0;
+    dbuf fftwork;
+
+    // current segment state for the stage entry points
+    exm_slot slot;
+    bool traj_ok = false, times_ok = false;
+    int cur_nwalk = 0;
+    float cur_lw = 0.f;
+    std::vector<exm_slot> slots;
+};
+
+// allocation with budget accounting
+void exm_alloc(exm_ctx *ctx, dbuf &b, size_t bytes);
+void exm_free(exm_ctx *ctx, dbuf &b);
+void exm_ensure(exm_ctx *ctx, dbuf &b, size_t bytes);   // grow-only

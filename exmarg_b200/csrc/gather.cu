@@ -1,0 +1,542 @@
+// The table read of Eq. (C7) (exmarg/search/gather.py:32-107) on the B200.
+//
+// k_gather_planes (the pe_intrinsic path): one block per (node k, lag r, block of up
+// to 2048 templates).  The block walks the 48 phase-plane pairs (p, p+1) of the
+// node's lag slab T[k, r]; for each plane it stages, with one TMA copy, a window of
+// 80 beta rows x 160 Delta columns into shared memory (three slots: two planes in
+// use, one in flight).  The descriptors of the lag are sorted by (plane pair,
+// template), and each warp owns a contiguous range of templates, so for each pair a
+// warp reads one contiguous run of 16-byte descriptors, evaluates the bilinear x
+// linear interpolation from shared memory, and merges the log-sum-exp of each
+// template with warp shuffles into a per-template accumulator that only it writes.
+// Values are carried as (B, e) with B a stored float32 table value and e a small
+// float32 correction, so a tap of size ~1e3 keeps ~1e-7 absolute precision.  Taps
+// outside the window, and taps whose beta is clamped to the table, take an exact
+// float64 path that reads the table from global memory.
+//
+// k_gather_simple (the gather_cpu / gather_gpu contract, any table per slot): one
+// block per (row, lag), the reference's arithmetic in float64.
+#include "common.cuh"
+#include "kernels.cuh"
+
+#define SLOT_FLOATS (EXM_WB * EXM_WD)
+#define SLOT_BYTES (SLOT_FLOATS * 4)
+#define EXM_WAIT_CYCLES (2000000000LL)   // about one second at 1.9 GHz
+
+struct PlaneArgs {
+    const uint4 *desc;
+    const int32_t *tside;
+    const int *off;
+    const float2 *H, *L;
+    const float *T;
+    const int *mlo, *mhi, *bnode, *win, *tau;
+    const double *boff, *cb, *ckd;
+    double *part;
+    unsigned *err;
+    long long tstride, per_lag;
+    int nn, ntau, nphif, nb, nd, ndp, nt, nmc, m_base, nm_total, r0;
+    float lw;
+    double rph, rdb, rdd, offd;
+    int cki[EXM_MAX_NODES];
+    float ckf[EXM_MAX_NODES];
+};
+
+// ------------------------------------------------------------------ TMA + mbarrier
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t *bar, float *dst, int x, int y, int z,
+                                               int w, int v, unsigned bytes)
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+        "[%7];" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(v), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// bounded wait on a phase of an mbarrier; false (and the error word set) if it ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err)
+{
+    const uint32_t a = smem_u32(bar);
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (clock64() - t0 > EXM_WAIT_CYCLES) {
+            atomicOr(err, EXM_DEVERR_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ log-sum-exp of (B, e) values
+
+__device__ __forceinline__ void lse_merge(float &B, float &E, float &S, float B2, float E2, float S2)
+{
+    const float d = (B2 - B) + (E2 - E);
+    if (d > 0.f) {
+        S = fmaf(S, __expf(-d), S2);
+        B = B2;
+        E = E2;
+    } else {
+        S = fmaf(S2, __expf(d), S);
+    }
+}
+
+// segmented reduction over lanes with equal id (ids non-decreasing along the lanes of a run);
+// afterwards the first lane of each run holds the run's total
+__device__ __forceinline__ bool seg_reduce(int id, float &B, float &E, float &S)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int id2 = __shfl_down_sync(0xffffffffu, id, o);
+        const float B2 = __shfl_down_sync(0xffffffffu, B, o);
+        const float E2 = __shfl_down_sync(0xffffffffu, E, o);
+        const float S2 = __shfl_down_sync(0xffffffffu, S, o);
+        if (lane + o < 32 && id2 == id) lse_merge(B, E, S, B2, E2, S2);
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, id, 1);
+    return lane == 0 || prev != id;
+}
+
+// bilinear in (beta, Delta) on planes p and p+1 of the staged windows, linear in phase;
+// value = t00 + eps with t00 the stored value at (p, b0, d0)
+__device__ __forceinline__ void interp_window(const float *s0, const float *s1, int o, float fbf, float fd, float w,
+                                              float &B, float &E)
+{
+    const float t00 = s0[o], t01 = s0[o + 1], t10 = s0[o + EXM_WD], t11 = s0[o + EXM_WD + 1];
+    const float u00 = s1[o], u01 = s1[o + 1], u10 = s1[o + EXM_WD], u11 = s1[o + EXM_WD + 1];
+    const float a0 = t01 - t00, c0 = t10 - t00, e0 = (t11 - t10) - a0;
+    const float eps0 = fmaf(fd, a0, fbf * fmaf(fd, e0, c0));
+    const float a1 = u01 - u00, c1 = u10 - u00, e1 = (u11 - u10) - a1;
+    const float eps1 = fmaf(fd, a1, fbf * fmaf(fd, e1, c1));
+    B = t00;
+    E = fmaf(w, (u00 - t00) + (eps1 - eps0), eps0);
+}
+
+__device__ __forceinline__ void split_double(double v, float &B, float &E)
+{
+    B = (float)v;
+    E = (float)(v - (double)B);
+}
+
+template <int NW>
+__global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    float *win = (float *)smem;
+    uint64_t *mbar = (uint64_t *)(smem + 3 * SLOT_BYTES);
+    float *aB = (float *)(smem + 3 * SLOT_BYTES + 64);
+    float *aE = aB + EXM_TCH, *aS = aE + EXM_TCH;
+    float *bB = aS + EXM_TCH, *bE = bB + EXM_TCH, *bS = bE + EXM_TCH;
+    float *bcf = bS + EXM_TCH;               // boundary offset, fraction
+    int *bci = (int *)(bcf + EXM_TCH);       // boundary offset, integer part
+    short *bslot = (short *)(bci + EXM_TCH);
+    __shared__ int scan_sh[33];
+
+    const int k = blockIdx.x % a.nn, rl = blockIdx.x / a.nn, r = a.r0 + rl;
+    const int lo0 = max(a.mlo[k], a.m_base), hi0 = min(a.mhi[k], a.m_base + a.nmc);
+    const int lo = lo0 + blockIdx.y * EXM_TCH;
+    const int hi = min(hi0, lo + EXM_TCH);
+    if (lo >= hi) return;
+    const int n = hi - lo;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // accumulators and the boundary-slot map (templates whose lowest point is node k)
+    int carry = 0;
+    for (int j0 = 0; j0 < n; j0 += NW * 32) {
+        const int j = j0 + tid;
+        const int isb = (j < n) && a.bnode[lo + j] == k;
+        int v = isb, x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) scan_sh[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int s = lane < NW ? scan_sh[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            if (lane < NW) scan_sh[lane] = s;
+        }
+        __syncthreads();
+        const int excl = carry + x - v + (warp ? scan_sh[warp - 1] : 0);
+        if (j < n) {
+            aB[j] = -1e30f;
+            aE[j] = 0.f;
+            aS[j] = 0.f;
+            bslot[j] = isb ? (short)excl : (short)-1;
+            if (isb) {
+                bB[excl] = -1e30f;
+                bE[excl] = 0.f;
+                bS[excl] = 0.f;
+                const double c = a.cb[lo + j];
+                const double f = floor(c);
+                bci[excl] = (int)f;
+                bcf[excl] = (float)(c - f);
+            }
+        }
+        carry += scan_sh[NW - 1];
+        __syncthreads();
+    }
+
+    const int C0 = a.win[0], R0 = a.win[1 + k];
+    const int cki = a.cki[k];
+    const float ckf = a.ckf[k];
+    if (tid == 0) {
+        for (int s = 0; s < 3; ++s) mbar_init(&mbar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        tma_load_plane(&tmap, &mbar[0], win, C0, R0, 0, r, k, SLOT_BYTES);
+        tma_load_plane(&tmap, &mbar[1], win + SLOT_FLOATS, C0, R0, 1, r, k, SLOT_BYTES);
+    }
+    int issued = 2;
+
+    const int wa = lo + (int)((long long)n * warp / NW), wb = lo + (int)((long long)n * (warp + 1) / NW);
+    const int ia = wa - a.m_base, ibd = wb - a.m_base;
+    const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
+    const uint4 *descr = a.desc + (long long)rl * a.per_lag;
+    const int32_t *tsr = a.tside + (long long)rl * a.per_lag;
+    const float *Tk = a.T + (long long)k * a.tstride;
+    const int nt = a.nt;
+    const int tau0 = ((a.tau[r] % nt) + nt) % nt;
+    const double ckd = a.ckd[k];
+
+    bool ok = mbar_wait(&mbar[0], 0, a.err);
+    for (int p = 0; p < EXM_NPAIR; ++p) {
+        if (p > 0) __syncthreads();   // every warp is done with plane p - 1: its slot can be refilled
+        if (tid == 0 && ok && p + 2 < a.nphif) {
+            const int q = p + 2;
+            tma_load_plane(&tmap, &mbar[q % 3], win + (q % 3) * SLOT_FLOATS, C0, R0, q, r, k, SLOT_BYTES);
+            ++issued;
+        }
+        ok = ok && mbar_wait(&mbar[(p + 1) % 3], ((p + 1) / 3) & 1, a.err);
+        if (!ok) continue;
+        const float *s0 = win + (p % 3) * SLOT_FLOATS, *s1 = win + ((p + 1) % 3) * SLOT_FLOATS;
+        const int beg = offr[p * (a.nmc + 1) + ia], end = offr[p * (a.nmc + 1) + ibd];
+        for (int j0 = beg; j0 < end; j0 += 32) {
+            const int j = j0 + lane;
+            const bool act = j < end;
+            uint4 q = make_uint4(0u, 0u, 0u, 0u);
+            if (act) q = __ldg(descr + j);
+            const int il = (int)(q.w >> 19);                  // chunk-local template
+            int tr = act ? il + a.m_base - lo : -1;           // template within the block
+            if (act && (unsigned)tr >= (unsigned)n) {         // a descriptor outside the warp's run: report, skip
+                atomicOr(a.err, EXM_DEVERR_BOUNDS);
+                tr = -1;
+            }
+            const bool use = act && tr >= 0;
+            const float fb = __uint_as_float(q.x), fd = __uint_as_float(q.y);
+            const float w = __uint_as_float(q.z & 0x7FFFFFFFu);
+            const float lwv = (q.z >> 31) ? a.lw : 0.f;
+            const int d0 = (int)((q.w >> 11) & 0xFFu);
+            const int ibh = ((int)(q.w << 21)) >> 21;
+            float vB = -1e30f, vE = 0.f, vS = 0.f;
+            if (use) {
+                const float sfr = fb + ckf;
+                const int cy = sfr >= 1.f;
+                const float fbf = cy ? sfr - 1.f : sfr;
+                const int b0 = ibh + cki + cy;
+                const int rb = b0 - R0, rd = d0 - C0;
+                const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
+                                  b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf > 0.999999f);
+                if (fast) {
+                    interp_window(s0, s1, rb * EXM_WD + rd, fbf, fd, w, vB, vE);
+                    vE += lwv;
+                } else {
+                    const int t = tsr[j];
+                    int i1 = t + tau0;
+                    if (i1 >= nt) i1 -= nt;
+                    const double v = exm_tap_fp64<float>(a.L[(long long)il * nt + t], a.H[(long long)il * nt + i1],
+                                                         ckd + a.boff[il + a.m_base], r, Tk, a.nphif, a.nb, a.nd,
+                                                         a.ndp, a.rph, a.rdb, a.rdd, a.offd);
+                    split_double(v, vB, vE);
+                    vE += lwv;
+                }
+                vS = 1.f;
+            }
+            // boundary point of the templates whose lowest point is this node
+            const int bs = use ? (int)bslot[tr] : -1;
+            float cB = -1e30f, cE = 0.f, cS = 0.f;
+            if (__any_sync(0xffffffffu, bs >= 0)) {
+                if (bs >= 0) {
+                    const float sfr = fb + bcf[bs];
+                    const int cy = sfr >= 1.f;
+                    const float fbf = cy ? sfr - 1.f : sfr;
+                    const int b0 = ibh + bci[bs] + cy;
+                    const int rb = b0 - R0, rd = d0 - C0;
+                    const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) &&
+                                      (unsigned)rd <= (unsigned)(EXM_WD - 2) && b0 <= a.nb - 2 &&
+                                      !(b0 == a.nb - 2 && fbf > 0.999999f);
+                    if (fast) {
+                        interp_window(s0, s1, rb * EXM_WD + rd, fbf, fd, w, cB, cE);
+                    } else {
+                        const int t = tsr[j];
+                        int i1 = t + tau0;
+                        if (i1 >= nt) i1 -= nt;
+                        const int gi = il + a.m_base;
+                        const double v = exm_tap_fp64<float>(a.L[(long long)il * nt + t], a.H[(long long)il * nt + i1],
+                                                             a.cb[gi] + a.boff[gi], r, Tk, a.nphif, a.nb, a.nd, a.ndp,
+                                                             a.rph, a.rdb, a.rdd, a.offd);
+                        split_double(v, cB, cE);
+                    }
+                    cE += lwv;
+                    cS = 1.f;
+                }
+                const bool hb = seg_reduce(bs >= 0 ? bs : -2 - lane, cB, cE, cS);
+                if (hb && bs >= 0) {
+                    float B = bB[bs], E = bE[bs], S = bS[bs];
+                    lse_merge(B, E, S, cB, cE, cS);
+                    bB[bs] = B;
+                    bE[bs] = E;
+                    bS[bs] = S;
+                }
+            }
+            const bool head = seg_reduce(tr, vB, vE, vS);
+            if (head && use) {
+                float B = aB[tr], E = aE[tr], S = aS[tr];
+                lse_merge(B, E, S, vB, vE, vS);
+                aB[tr] = B;
+                aE[tr] = E;
+                aS[tr] = S;
+            }
+        }
+    }
+    __syncthreads();
+    // drain: every issued copy has landed before the block exits (bounded)
+    if (!ok && tid == 0) {
+        // the newest copy of each slot completes after the older ones of that slot
+        for (int q = max(0, issued - 3); q < issued; ++q) mbar_wait(&mbar[q % 3], (q / 3) & 1, a.err);
+    }
+    for (int j = tid; j < n; j += NW * 32) {
+        const float S = aS[j];
+        const double v = (ok && S > 0.f) ? (double)aB[j] + (double)aE[j] + log((double)S) : -INFINITY;
+        a.part[((long long)k * a.ntau + r) * a.nm_total + lo + j] = v;
+        const int bs = bslot[j];
+        if (bs >= 0) {
+            const float S2 = bS[bs];
+            const double v2 = (ok && S2 > 0.f) ? (double)bB[bs] + (double)bE[bs] + log((double)S2) : -INFINITY;
+            a.part[((long long)a.nn * a.ntau + r) * a.nm_total + lo + j] = v2;
+        }
+    }
+}
+
+#define GATHER_NW 16
+
+static size_t planes_smem()
+{
+    return (size_t)3 * SLOT_BYTES + 64 + (size_t)EXM_TCH * (8 * 4 + 2);
+}
+
+void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc)
+{
+    if (!ctx->tmap_ok) EXM_THROW(EXM_ERR_STATE, "tensor map of the store is not set");
+    PlaneArgs a;
+    memset(&a, 0, sizeof(a));
+    a.desc = (const uint4 *)sl.desc.p;
+    a.tside = (const int32_t *)sl.tside.p;
+    a.off = (const int *)sl.cnt.p;
+    a.H = (const float2 *)sl.traj.p;
+    a.L = a.H + (size_t)ci.nmc * ctx->nt;
+    a.T = (const float *)ctx->T.p;
+    a.mlo = (const int *)ctx->d_mlo.p;
+    a.mhi = (const int *)ctx->d_mhi.p;
+    a.bnode = (const int *)ctx->d_bnode.p;
+    a.win = (const int *)sl.win.p;
+    a.tau = (const int *)ctx->d_tau.p;
+    a.boff = (const double *)ctx->d_bhat_off.p;
+    a.cb = (const double *)ctx->d_cb.p;
+    a.ckd = (const double *)ctx->d_ckd.p;
+    a.part = (double *)sl.part.p;
+    a.err = (unsigned *)sl.dev_err.p;
+    a.tstride = (long long)ctx->tstride;
+    a.per_lag = (long long)ci.nmc * ci.nwalk;
+    a.nn = ctx->nn;
+    a.ntau = ctx->ntau;
+    a.nphif = ctx->nphif;
+    a.nb = ctx->nb;
+    a.nd = ctx->nd;
+    a.ndp = ctx->ndp;
+    a.nt = ctx->nt;
+    a.nmc = ci.nmc;
+    a.m_base = ci.m_base;
+    a.nm_total = ctx->nm;
+    a.r0 = r0;
+    a.lw = ci.lw;
+    a.rph = EXM_NPHI / 6.283185307179586;
+    a.rdb = 2.0 / ctx->dbeta;
+    a.rdd = 1.0 / ctx->ddelta;
+    a.offd = -ctx->delta0 / ctx->ddelta;
+    for (int k = 0; k < ctx->nn; ++k) {
+        const double f = std::floor(ctx->ck[k]);
+        a.cki[k] = (int)f;
+        a.ckf[k] = (float)(ctx->ck[k] - f);
+    }
+    // blocks of up to EXM_TCH templates: as many as the widest node range needs
+    int maxn = 0;
+    for (int k = 0; k < ctx->nn; ++k) {
+        const int lo = std::max(ctx->mlo[k], ci.m_base), hi = std::min(ctx->mhi[k], ci.m_base + ci.nmc);
+        maxn = std::max(maxn, hi - lo);
+    }
+    if (maxn <= 0) return;
+    const size_t smem = planes_smem();
+    EXM_CUDA(cudaFuncSetAttribute(k_gather_planes<GATHER_NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(rc * ctx->nn, (maxn + EXM_TCH - 1) / EXM_TCH);
+    k_gather_planes<GATHER_NW><<<grid, GATHER_NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+    EXM_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------ the general gather contract, float64
+
+struct SimpleArgs {
+    const float2 *H, *L;
+    const int32_t *sel;
+    const float *T;
+    const int *rows, *tab, *tau;
+    const double *lna;
+    double *om, *os;
+    long long tstride;
+    int nt, nwalk, use_sel, ns, nsel, nphif, nb, nd, ndp, ntau;
+    float lw;
+    double beta0, dbeta, rph, rdb, rdd, offd;
+};
+
+__global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
+{
+    __shared__ double shm[8], shs[8];
+    const int j = blockIdx.x, r = blockIdx.y;
+    const int row = a.rows[j];
+    const int nt = a.nt;
+    const int tau0 = ((a.tau[r] % nt) + nt) % nt;
+    const float2 *H = a.H + (long long)row * nt, *L = a.L + (long long)row * nt;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int n = 0; n < a.ns; ++n) {
+        const float *Tn = a.T + (long long)a.tab[j * a.ns + n] * a.tstride;
+        const double offb = (a.lna[j * a.ns + n] - a.beta0) / a.dbeta;
+        double m = -1e300, s = 0.0;
+        for (int kk = threadIdx.x; kk < a.nwalk; kk += blockDim.x) {
+            int t = kk, flag = 0;
+            if (a.use_sel) {
+                const int v = a.sel[(long long)row * a.nwalk + kk];
+                t = v & 0x7FFFFFFF;
+                flag = (unsigned)v >> 31;
+            }
+            int i1 = t + tau0;
+            if (i1 >= nt) i1 -= nt;
+            double acc = exm_tap_fp64<float>(L[t], H[i1], offb, r, Tn, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
+                                             a.rdd, a.offd);
+            if (a.use_sel) acc += flag ? (double)a.lw : 0.0;
+            if (acc > m) {
+                s = s * exp(m - acc) + 1.0;
+                m = acc;
+            } else {
+                s += exp(acc - m);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double m2 = __shfl_down_sync(0xffffffffu, m, o), s2 = __shfl_down_sync(0xffffffffu, s, o);
+            if (m2 > m) {
+                s = s2 + s * exp(m - m2);
+                m = m2;
+            } else {
+                s = s + s2 * exp(m2 - m);
+            }
+        }
+        if (lane == 0) {
+            shm[warp] = m;
+            shs[warp] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double M = shm[0], S = shs[0];
+            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+                if (shm[q] > M) {
+                    S = shs[q] + S * exp(M - shm[q]);
+                    M = shm[q];
+                } else {
+                    S = S + shs[q] * exp(shm[q] - M);
+                }
+            }
+            const long long o = ((long long)n * a.ntau + r) * a.nsel + j;
+            a.om[o] = M;
+            a.os[o] = S;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_lse_lags(const double *om, const double *os, int ns, int ntau, int nsel, int nt, double *out)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= ns * nsel) return;
+    const int n = idx / nsel, j = idx - n * nsel;
+    double mx = -INFINITY;
+    for (int r = 0; r < ntau; ++r) mx = fmax(mx, om[((long long)n * ntau + r) * nsel + j]);
+    double tot = 0.0;
+    for (int r = 0; r < ntau; ++r) {
+        const long long o = ((long long)n * ntau + r) * nsel + j;
+        tot += os[o] * exp(om[o] - mx);
+    }
+    out[idx] = mx + log(tot) - log((double)nt);
+}
+
+void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const int *d_rows, const int *d_tab,
+                           const double *d_lna, int nwalk, int use_sel, float lw, double *d_out)
+{
+    SimpleArgs a;
+    a.H = (const float2 *)sl.traj.p;
+    a.L = a.H + (size_t)ctx->nm * ctx->nt;
+    a.sel = (const int32_t *)sl.sel.p;
+    a.T = (const float *)ctx->T.p;
+    a.rows = d_rows;
+    a.tab = d_tab;
+    a.tau = (const int *)ctx->d_tau.p;
+    a.lna = d_lna;
+    a.om = (double *)sl.part.p;
+    a.os = a.om + (size_t)ns * ctx->ntau * nsel;
+    a.tstride = (long long)ctx->tstride;
+    a.nt = ctx->nt;
+    a.nwalk = nwalk;
+    a.use_sel = use_sel;
+    a.ns = ns;
+    a.nsel = nsel;
+    a.nphif = ctx->nphif;
+    a.nb = ctx->nb;
+    a.nd = ctx->nd;
+    a.ndp = ctx->ndp;
+    a.ntau = ctx->ntau;
+    a.lw = lw;
+    a.beta0 = ctx->beta0;
+    a.dbeta = ctx->dbeta;
+    a.rph = EXM_NPHI / 6.283185307179586;
+    a.rdb = 2.0 / ctx->dbeta;
+    a.rdd = 1.0 / ctx->ddelta;
+    a.offd = -ctx->delta0 / ctx->ddelta;
+    dim3 grid(nsel, ctx->ntau);
+    k_gather_simple<<<grid, 256, 0, ctx->stream>>>(a);
+    k_lse_lags<<<(ns * nsel + 255) / 256, 256, 0, ctx->stream>>>(a.om, a.os, ns, ctx->ntau, nsel, ctx->nt, d_out);
+    EXM_CUDA(cudaGetLastError());
+}

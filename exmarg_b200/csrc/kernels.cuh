@@ -1,0 +1,126 @@
+// Device helpers shared by the kernels, and the host-side launchers of each stage.
+#pragma once
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+
+// staging window of one (node, lag, phase plane): rows of beta x columns of Delta
+#define EXM_WB 80
+#define EXM_WD 160
+#define EXM_TCH 2048        // templates per gather block
+#define EXM_MAX_CHUNK 8192  // templates per pass (13-bit template field of a descriptor)
+#define EXM_MAX_NODES 64
+#define EXM_HB_LO (-1024)   // beta-hat histogram covers [-1024, 1024)
+#define EXM_HB_N 2048
+
+struct TapGeom {
+    double rph;   // NPHI / (2 pi)
+    double rdb;   // 2 / dbeta
+    double rdd;   // 1 / ddelta
+    double offd;  // -delta0 / ddelta
+    int nd, nt;
+};
+
+// The per-tap quantities that do not depend on the node (the reference computes
+// them per node, exmarg/search/gather.py:50-82): the plane pair p and the weight w
+// of plane p + 1, beta-hat = ln|z_L| 2/dbeta - ln(u)/dbeta as floor + fraction,
+// and the Delta coordinate of the unclamped-beta case as (d0, fd).
+__device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, double boff, const TapGeom &g, int &p, float &w,
+                                             int &ib, float &fb, int &d0, float &fd)
+{
+    double x3 = (double)(h.y - l.y) * g.rph;   // float32 difference, float64 scale, as the reference
+    if (x3 < 0.0) x3 += EXM_NPHI;
+    if (x3 >= EXM_NPHI) x3 -= EXM_NPHI;
+    int c0 = (int)x3;
+    c0 = c0 < 0 ? 0 : (c0 > EXM_NPHI - 1 ? EXM_NPHI - 1 : c0);
+    const double fc = x3 - c0;
+    // planes ci0 = reflect(c0) and ci1 = reflect(c0 + 1) are always {p, p + 1}
+    if (c0 <= EXM_NPAIR - 1) {
+        p = c0;
+        w = (float)fc;
+    } else {
+        p = EXM_NPHI - 1 - c0;
+        w = (float)(1.0 - fc);
+    }
+    const double bh = (double)l.x * g.rdb + boff;
+    const double fl = floor(bh);
+    ib = (int)fmax(fmin(fl, 1023.0), -1024.0);
+    fb = (float)(bh - fl);
+    double xd = ((double)h.x - (double)l.x) * g.rdd + g.offd;
+    if (xd < 0.0) xd = 0.0; else if (xd > g.nd - 1 - 1e-6) xd = g.nd - 1 - 1e-6;
+    d0 = (int)xd;
+    fd = (float)(xd - d0);
+}
+
+// the reference's tap value in float64 (exmarg/search/gather.py:50-93) for one
+// node table Tn (padded rows of ndp floats), lag row r; lw added by the caller
+template <typename TT>
+__device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, int r, const TT *__restrict__ Tn,
+                                               int nphif, int nb, int nd, int ndp, double rph, double rdb, double rdd,
+                                               double offd);
+
+__device__ __forceinline__ float exm_ld(const float *p) { return __ldg(p); }
+
+template <>
+__device__ __forceinline__ double exm_tap_fp64<float>(float2 l, float2 h, double offb, int r,
+                                                      const float *__restrict__ Tn, int nphif, int nb, int nd, int ndp,
+                                                      double rph, double rdb, double rdd, double offd)
+{
+    double x3 = (double)(h.y - l.y) * rph;
+    if (x3 < 0.0) x3 += EXM_NPHI;
+    if (x3 >= EXM_NPHI) x3 -= EXM_NPHI;
+    int c0 = (int)x3;
+    c0 = c0 < 0 ? 0 : (c0 > EXM_NPHI - 1 ? EXM_NPHI - 1 : c0);
+    const double fc = x3 - c0;
+    const int c1 = (c0 + 1) % EXM_NPHI;
+    const double aH = h.x, aL = l.x;
+    const double xbr = aL * rdb + offb;
+    double xb = xbr;
+    if (xb < 0.0) xb = 0.0; else if (xb > nb - 1 - 1e-6) xb = nb - 1 - 1e-6;
+    const double aLc = aL + (xb - xbr) / rdb;
+    double xd = (aH - aLc) * rdd + offd;
+    if (xd < 0.0) xd = 0.0; else if (xd > nd - 1 - 1e-6) xd = nd - 1 - 1e-6;
+    const int d0 = (int)xd;
+    const double fdf = xd - d0, fd0 = 1.0 - fdf;
+    const int d1 = d0 + 1 < nd ? d0 + 1 : nd - 1;
+    const int b0 = (int)xb;
+    const double fbf = xb - b0, fb0 = 1.0 - fbf;
+    const int b1 = b0 + 1 < nb ? b0 + 1 : nb - 1;
+    double acc = 0.0;
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+        int ci = cc ? c1 : c0;
+        if (ci > EXM_NPHI / 2) ci = EXM_NPHI - ci;
+        const double fci = cc ? fc : 1.0 - fc;
+        const float *r0 = Tn + (((long long)r * nphif + ci) * nb + b0) * ndp;
+        const float *r1 = Tn + (((long long)r * nphif + ci) * nb + b1) * ndp;
+        const double v = fb0 * (fd0 * (double)exm_ld(r0 + d0) + fdf * (double)exm_ld(r0 + d1)) +
+                         fbf * (fd0 * (double)exm_ld(r1 + d0) + fdf * (double)exm_ld(r1 + d1));
+        acc += fci * v;
+    }
+    return acc;
+}
+
+// ------------------------------------------------------------------ launchers
+
+void exm_fft_plan(exm_ctx *ctx, int batch);
+void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm);
+void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S);
+void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
+
+struct ChunkInfo {
+    int m_base;   // first internal template of the chunk
+    int nmc;      // templates in the chunk
+    int nwalk;    // walked times per template (n_time when every time is walked)
+    int use_sel;  // sel holds the walked times
+    float lw;     // log weight of a random draw
+};
+void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc, bool first_chunk_of_lags);
+void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc);
+void exm_run_node_lse(exm_ctx *ctx, exm_slot &sl, int m_base, int nmc);
+void exm_run_lnb(exm_ctx *ctx, exm_slot &sl);
+void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const int *d_rows, const int *d_tab,
+                           const double *d_lna, int nwalk, int use_sel, float lw, double *d_out);
+void exm_run_distance_weights(exm_ctx *ctx, double ymin, int prior, const double *d_lny, const double *d_p,
+                              int n_dens);

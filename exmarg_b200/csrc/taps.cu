@@ -1,0 +1,251 @@
+// Tap descriptors for the plane-staged gather.
+//
+// A tap is one (template, walked time, lag).  Its plane pair p, the weight of plane
+// p + 1, beta-hat and the Delta coordinate do not depend on the node, so they are
+// computed once per tap (in float64, as the reference computes them per node) and
+// packed into 16 bytes:
+//   x = fb (float, fraction of beta-hat), y = fd (float, fraction of Delta),
+//   z = w (float, weight of plane p + 1) | bit 31: the time is a random draw,
+//   w = template (13 bits) << 19 | d0 (8 bits) << 11 | floor(beta-hat) (11 bits, signed).
+// For each lag the descriptors are counting-sorted by (p, template), so every node's
+// gather block reads, for each plane pair it has staged, one contiguous run per warp.
+// A second array holds each descriptor's time index for the exact slow path.
+#include "common.cuh"
+#include "kernels.cuh"
+
+struct TapArgs {
+    const float2 *H, *L;
+    const int32_t *sel;
+    const double *boff;   // [nmc] -ln(u)/dbeta of the chunk's templates
+    const int *tau;       // [ntau]
+    int *cnt;             // [rc][48][nmc + 1]
+    int *hist_b;          // [EXM_HB_N]
+    int *hist_d;          // [256]
+    uint4 *desc;
+    int32_t *tside;
+    TapGeom g;
+    int nmc, nwalk, use_sel, r0, want_hb;
+    long long per_lag;    // nmc * nwalk
+};
+
+__device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t, int &flag)
+{
+    if (a.use_sel) {
+        const int v = a.sel[(long long)i * a.nwalk + k];
+        t = v & 0x7FFFFFFF;
+        flag = (unsigned)v >> 31;
+    } else {
+        t = k;
+        flag = 0;
+    }
+}
+
+// counts per (lag, pair, template), and the histograms that place the staging windows
+__global__ void __launch_bounds__(256) k_tap_count(TapArgs a)
+{
+    __shared__ int c[EXM_NPAIR];
+    __shared__ int hd[256];
+    __shared__ int hb[EXM_HB_N];
+    const int i = blockIdx.x, rl = blockIdx.y;
+    const bool do_hb = a.want_hb && rl == 0;
+    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) c[q] = 0;
+    for (int q = threadIdx.x; q < 256; q += blockDim.x) hd[q] = 0;
+    if (do_hb)
+        for (int q = threadIdx.x; q < EXM_HB_N; q += blockDim.x) hb[q] = 0;
+    __syncthreads();
+    const int nt = a.g.nt;
+    const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
+    const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
+    const double boff = a.boff[i];
+    for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
+        int t, flag;
+        tap_time(a, i, k, t, flag);
+        int i1 = t + tau0;
+        if (i1 >= nt) i1 -= nt;
+        int p, ib, d0;
+        float w, fb, fd;
+        exm_tap_geom(L[t], H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+        atomicAdd(&c[p], 1);
+        atomicAdd(&hd[d0], 1);
+        if (do_hb) atomicAdd(&hb[ib - EXM_HB_LO], 1);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x)
+        a.cnt[((long long)rl * EXM_NPAIR + q) * (a.nmc + 1) + i] = c[q];
+    for (int q = threadIdx.x; q < 256; q += blockDim.x)
+        if (hd[q]) atomicAdd(&a.hist_d[q], hd[q]);
+    if (do_hb)
+        for (int q = threadIdx.x; q < EXM_HB_N; q += blockDim.x)
+            if (hb[q]) atomicAdd(&a.hist_b[q], hb[q]);
+}
+
+// exclusive scan over (pair, template) per lag: cnt becomes the start offsets; column
+// nmc of pair p is the start of pair p + 1
+__global__ void __launch_bounds__(1024) k_tap_scan(int *cnt, int nmc)
+{
+    __shared__ int sh[33];
+    const int rl = blockIdx.x;
+    int *c = cnt + (long long)rl * EXM_NPAIR * (nmc + 1);
+    const int n = EXM_NPAIR * nmc;
+    int carry = 0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int e = base + threadIdx.x;
+        const int p = e / nmc, i = e - p * nmc;
+        const int v = (e < n) ? c[p * (nmc + 1) + i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int s = sh[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            sh[lane] = s;
+        }
+        __syncthreads();
+        const int excl = carry + x - v + (warp ? sh[warp - 1] : 0);
+        if (e < n) c[p * (nmc + 1) + i] = excl;
+        const int tot = sh[31];
+        __syncthreads();
+        carry += tot;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < EXM_NPAIR; p += blockDim.x)
+        c[p * (nmc + 1) + nmc] = (p + 1 < EXM_NPAIR) ? c[(p + 1) * (nmc + 1)] : carry;
+}
+
+// descriptors, stably scattered to their (lag, pair, template) runs
+__global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a)
+{
+    __shared__ int wcnt[8][EXM_NPAIR];
+    __shared__ int base[EXM_NPAIR];
+    const int i = blockIdx.x, rl = blockIdx.y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nt = a.g.nt;
+    const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
+    const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
+    const double boff = a.boff[i];
+    const int *off = a.cnt + (long long)rl * EXM_NPAIR * (a.nmc + 1);
+    uint4 *desc = a.desc + (long long)rl * a.per_lag;
+    int32_t *tside = a.tside + (long long)rl * a.per_lag;
+    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) base[q] = off[q * (a.nmc + 1) + i];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int k0 = 0; k0 < a.nwalk; k0 += blockDim.x) {
+        for (int q = threadIdx.x; q < 8 * EXM_NPAIR; q += blockDim.x) (&wcnt[0][0])[q] = 0;
+        __syncthreads();
+        const int k = k0 + threadIdx.x;
+        int p = -1, t = 0, flag = 0, ib = 0, d0 = 0;
+        float w = 0.f, fb = 0.f, fd = 0.f;
+        if (k < a.nwalk) {
+            tap_time(a, i, k, t, flag);
+            int i1 = t + tau0;
+            if (i1 >= nt) i1 -= nt;
+            exm_tap_geom(L[t], H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, p);
+        const int rk = __popc(peers & lt);
+        if (p >= 0 && rk == 0) wcnt[warp][p] = __popc(peers);
+        __syncthreads();
+        int pos = 0;
+        if (p >= 0) {
+            int pre = 0;
+            for (int ww = 0; ww < warp; ++ww) pre += wcnt[ww][p];
+            pos = base[p] + pre + rk;
+        }
+        __syncthreads();
+        if (threadIdx.x < EXM_NPAIR) {
+            int s = 0;
+            for (int ww = 0; ww < 8; ++ww) s += wcnt[ww][threadIdx.x];
+            base[threadIdx.x] += s;
+        }
+        if (p >= 0 && pos >= 0 && pos < a.per_lag) {
+            uint4 d;
+            d.x = __float_as_uint(fb);
+            d.y = __float_as_uint(fd);
+            d.z = __float_as_uint(w) | ((unsigned)flag << 31);
+            d.w = ((unsigned)i << 19) | ((unsigned)d0 << 11) | ((unsigned)ib & 0x7FFu);
+            desc[pos] = d;
+            tside[pos] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// staging-window origins: column C0 (a multiple of 4) and, per node, the first beta row
+__global__ void k_windows(const int *hist_b, const int *hist_d, const int *cki, int nn, int nb, int nd, int ndp,
+                          int *win)
+{
+    __shared__ long long best[2];
+    if (threadIdx.x == 0) best[0] = best[1] = 0;
+    __syncthreads();
+    // columns: d0 in [C0, C0 + WD - 2]
+    const int cmax = max(0, ndp - EXM_WD);
+    for (int c0 = threadIdx.x * 4; c0 <= cmax; c0 += blockDim.x * 4) {
+        long long s = 0;
+        for (int d = c0; d <= min(c0 + EXM_WD - 2, nd - 1); ++d) s += hist_d[d];
+        long long key = (s << 12) | (4095 - (c0 >> 2));
+        atomicMax((unsigned long long *)&best[0], (unsigned long long)key);
+    }
+    // beta-hat rows: ib in [Rh, Rh + WB - 3]
+    for (int rh = threadIdx.x; rh < EXM_HB_N; rh += blockDim.x) {
+        long long s = 0;
+        for (int x = rh; x <= min(rh + EXM_WB - 3, EXM_HB_N - 1); ++x) s += hist_b[x];
+        long long key = (s << 12) | (4095 - rh);
+        atomicMax((unsigned long long *)&best[1], (unsigned long long)key);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        win[0] = (4095 - (int)(best[0] & 4095)) * 4;
+        const int rh = (4095 - (int)(best[1] & 4095)) + EXM_HB_LO;
+        for (int k = 0; k < nn; ++k) {
+            int r0 = rh + cki[k];
+            r0 = max(0, min(r0, nb - EXM_WB));
+            win[1 + k] = r0;
+        }
+    }
+}
+
+void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc, bool first_chunk_of_lags)
+{
+    const int nt = ctx->nt;
+    TapArgs a;
+    a.H = (const float2 *)sl.traj.p;
+    a.L = a.H + (size_t)ci.nmc * nt;
+    a.sel = (const int32_t *)sl.sel.p;
+    a.boff = (const double *)ctx->d_bhat_off.p + ci.m_base;
+    a.tau = (const int *)ctx->d_tau.p;
+    a.cnt = (int *)sl.cnt.p;
+    a.hist_b = (int *)sl.hist.p;
+    a.hist_d = a.hist_b + EXM_HB_N;
+    a.desc = (uint4 *)sl.desc.p;
+    a.tside = (int32_t *)sl.tside.p;
+    a.g.rph = EXM_NPHI / 6.283185307179586;
+    a.g.rdb = 2.0 / ctx->dbeta;
+    a.g.rdd = 1.0 / ctx->ddelta;
+    a.g.offd = -ctx->delta0 / ctx->ddelta;
+    a.g.nd = ctx->nd;
+    a.g.nt = nt;
+    a.nmc = ci.nmc;
+    a.nwalk = ci.nwalk;
+    a.use_sel = ci.use_sel;
+    a.r0 = r0;
+    a.want_hb = first_chunk_of_lags ? 1 : 0;
+    a.per_lag = (long long)ci.nmc * ci.nwalk;
+    if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
+    EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
+    dim3 grid(ci.nmc, rc);
+    k_tap_count<<<grid, 256, 0, ctx->stream>>>(a);
+    k_tap_scan<<<rc, 1024, 0, ctx->stream>>>(a.cnt, ci.nmc);
+    k_tap_scatter<<<grid, 256, 0, ctx->stream>>>(a);
+    k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
+                                          (int *)sl.win.p);
+    EXM_CUDA(cudaGetLastError());
+}

@@ -1,0 +1,118 @@
+"""The table store (the contract of exmarg/search/store.py:90-127).
+
+load_redshift_store reads every bd_*.npz node of a store directory (T (tau, phi+,
+beta, Delta) float32, beta, delta, tau_idx, alpha, s_node), sorted by s_node, into
+host memory (or maps them with mmap=True), exactly like the reference.  For
+device='b200' the tables are copied once into HBM by the analysis context and
+stay resident for every later call (upload_store); there is no per-call upload.
+"""
+
+import glob
+import os
+import struct
+import zipfile
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+NPHI = 96
+
+
+def _member_offset(path, name):
+    info = zipfile.ZipFile(path).getinfo(name)
+    if info.compress_type != 0:
+        raise ValueError("member %s of %s is compressed" % (name, path))
+    with open(path, "rb") as fh:
+        fh.seek(info.header_offset)
+        nlen, elen = struct.unpack("<HH", fh.read(30)[26:30])
+        fh.seek(info.header_offset + 30 + nlen + elen)
+        ver = np.lib.format.read_magic(fh)
+        rd = np.lib.format.read_array_header_1_0 if ver == (1, 0) else np.lib.format.read_array_header_2_0
+        shape, fortran, dtype = rd(fh)
+        return fh.tell(), shape, fortran, dtype
+
+
+def read_npz_member(path, name):
+    """one uncompressed .npy member of an npz, read sequentially"""
+    off, shape, fortran, dtype = _member_offset(path, name)
+    with open(path, "rb") as fh:
+        fh.seek(off)
+        arr = np.fromfile(fh, dtype=dtype, count=int(np.prod(shape)))
+    return arr.reshape(shape, order="F" if fortran else "C")
+
+
+def map_npz_member(path, name):
+    """read-only memory map of one uncompressed .npy member of an npz"""
+    off, shape, fortran, dtype = _member_offset(path, name)
+    return np.asarray(np.memmap(path, dtype=dtype, mode="r", offset=off, shape=shape, order="F" if fortran else "C"))
+
+
+@dataclass
+class RedshiftStore:
+    """signal power nodes s (sorted), amplitude-axis limits, grids, host tables and the truncation order"""
+    s: np.ndarray
+    alpha_lo: np.ndarray
+    alpha_hi: np.ndarray
+    beta: list
+    delta: list
+    tau_idx: np.ndarray
+    tables: list
+    n_max: int
+    device_tokens: dict = field(default_factory=dict, repr=False)
+
+
+def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False):
+    """every node of the store in host memory (about 0.75 GB per node at the production shape);
+    pinned is accepted for the reference's signature (the b200 path copies each table to HBM once)"""
+    files = glob.glob(os.path.join(store_dir, "bd_*.npz"))
+    if not files:
+        raise FileNotFoundError("no bd_*.npz in %s" % store_dir)
+    head = []
+    for f in files:
+        with np.load(f) as h:
+            head.append((float(h["s_node"]), float(h["alpha"][0]), float(h["alpha"][-1]), h["beta"], h["delta"],
+                         h["tau_idx"], f))
+    head.sort(key=lambda r: r[0])
+    s, alo, ahi, beta, delta, tau, files = zip(*head)
+    if mmap:
+        tables = [map_npz_member(f, "T.npy") for f in files]
+    else:
+        with ThreadPoolExecutor(max_workers=max(1, int(readers))) as ex:
+            tables = list(ex.map(lambda f: read_npz_member(f, "T.npy"), files))
+    return RedshiftStore(s=np.array(s), alpha_lo=np.array(alo), alpha_hi=np.array(ahi), beta=list(beta),
+                         delta=list(delta), tau_idx=tau[0], tables=tables,
+                         n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]))
+
+
+def store_grid(store):
+    """(beta0, dbeta, delta0, ddelta) shared by every node; the device path needs one grid"""
+    b0, d0 = np.asarray(store.beta[0], float), np.asarray(store.delta[0], float)
+    for b, d in zip(store.beta, store.delta):
+        if b.shape != b0.shape or d.shape != d0.shape or not (np.allclose(b, b0, rtol=0, atol=1e-12)
+                                                               and np.allclose(d, d0, rtol=0, atol=1e-12)):
+            raise ValueError("device 'b200' needs the same (beta, Delta) grids at every node")
+    return float(b0[0]), float(b0[1] - b0[0]), float(d0[0]), float(d0[1] - d0[0])
+
+
+def upload_store(store, ctx):
+    """copy the store's tables into the context's HBM once (skipped if this store is already resident)"""
+    token = id(store)
+    if ctx.store_token == token:
+        return
+    shape = tuple(np.asarray(store.tables[0]).shape)
+    beta0, dbeta, delta0, ddelta = store_grid(store)
+    ctx.store_init(len(store.tables), shape, store.tau_idx, beta0, dbeta, delta0, ddelta)
+    gen = getattr(store, "generator", None)
+    for k, T in enumerate(store.tables):
+        if gen is not None and T is None:
+            M, P, Q, S, seed = gen
+            ctx.store_generate_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], M, P, Q, S[k], seed)
+        else:
+            if tuple(np.asarray(T).shape) != shape:
+                raise ValueError("every node table must have the same shape")
+            ctx.store_set_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], T)
+    ctx.store_token = token
+    ctx.prep_token = None

@@ -1,0 +1,157 @@
+/*
+ * exmarg_b200 -- C ABI of libexmarg_b200.so, the B200 (sm_100a) implementation of
+ * exmarg's Eq. (C7) analysis path: matched filter -> table gather / log-sum-exp
+ * -> distance-prior quadrature.
+ *
+ * Plain pointers and sizes only.  Host arrays are caller-owned and borrowed for
+ * the duration of the call.  Device tables, banks and workspaces are owned by the
+ * context, which enforces its HBM budget.  Every entry point returns an int
+ * status (EXM_OK = 0); the message of the last failure is exm_last_error(ctx).
+ * Calls on one context are serialised by the caller (one context = one stream).
+ *
+ * Each entry point names the reference interface it replaces (paths relative to
+ * the reference repository).
+ */
+#ifndef EXMARG_B200_H
+#define EXMARG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define EXM_API __attribute__((visibility("default")))
+#else
+#define EXM_API
+#endif
+
+#define EXM_OK 0
+#define EXM_ERR_ARG 1     /* bad shape or argument      -> ValueError   */
+#define EXM_ERR_OOM 2     /* HBM budget or allocation   -> MemoryError  */
+#define EXM_ERR_CUDA 3    /* CUDA or cuFFT failure      -> RuntimeError */
+#define EXM_ERR_TIMEOUT 4 /* a bounded device wait ran out -> RuntimeError */
+#define EXM_ERR_STATE 5   /* call order (no store, no bank, no prepare) -> RuntimeError */
+
+#define EXM_DTYPE_F32 0
+#define EXM_DTYPE_F16 1
+#define EXM_DTYPE_BF16 2
+
+#define EXM_PRIOR_VOLUME 0
+#define EXM_PRIOR_TABULATED 1 /* a density of ln y on a grid ('madau-dickinson') */
+
+typedef struct exm_ctx exm_ctx;
+
+/* ------------------------------------------------------------------ context */
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+EXM_API int exm_version(void);
+
+/* One analysis context on CUDA device `device` with at most `hbm_budget` bytes of
+ * device memory (0: 90% of the free memory).  Replaces the implicit cupy device
+ * state of exmarg/search/bank.py:17-24 (array_module) and the memory fit of
+ * exmarg/search/pe.py:37-50 (_fit_chunk). */
+EXM_API int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out);
+EXM_API void exm_ctx_destroy(exm_ctx *ctx);
+EXM_API const char *exm_last_error(const exm_ctx *ctx);
+/* Bytes of device memory the context holds now. */
+EXM_API size_t exm_ctx_bytes(const exm_ctx *ctx);
+
+/* ------------------------------------------------------------------ store */
+
+/* Declare the store: n_nodes tables of shape (ntau, nphif, nb, nd), stored on the
+ * device as `dtype` (EXM_DTYPE_*), lags tau_idx (ntau, in samples), the (beta,
+ * Delta) grids beta0 + i dbeta and delta0 + j ddelta shared by every node.
+ * Replaces exmarg/search/store.py:204-214 (upload) with resident device tables. */
+EXM_API int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, int nb, int nd, int dtype,
+                   const int64_t *tau_idx, double beta0, double dbeta, double delta0, double ddelta);
+
+/* Node k: its signal power s and amplitude-axis limits (alpha[0], alpha[-1]), and
+ * its float32 table T (ntau, nphif, nb, nd, C order) copied from the host.
+ * Replaces one iteration of exmarg/search/store.py:210-212 and the per-node
+ * metadata of load_redshift_store (store.py:184-201). */
+EXM_API int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *T);
+
+/* Node k filled on the device by the seeded synthetic generator (the same float32
+ * values as exmarg_b200.synth.gen_table_node): T = M[b,d] * P[c] * Q[r] - S + hash
+ * perturbation.  M (nb*nd), P (nphif), Q (ntau) float32.  No reference
+ * counterpart: it stands in for reading bd_*.npz (store.py:149-168). */
+EXM_API int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi,
+                            const float *M, const float *P, const float *Q, float S, uint32_t seed);
+
+/* Copy node k back to the host as float32 (ntau, nphif, nb, nd) (decoded for
+ * 16-bit storage).  For tests. */
+EXM_API int exm_store_get_node(exm_ctx *ctx, int k, float *T_out);
+
+/* ------------------------------------------------------------------ bank */
+
+/* The template bank: nm templates of nfreq complex64 factors W = a e^{i psi0}
+ * (interleaved re, im), starting at frequency bin `lo` of a grid whose filter
+ * length is n_time = 8 nu_max; u (nm) the template powers; M, q, chi (nm) the
+ * bank axes (for the cell weights of ln B).  Replaces the device copy of
+ * exmarg/search/bank.py:35-54 (MassBank.__init__). */
+EXM_API int exm_bank_set(exm_ctx *ctx, int nm, int nfreq, int lo, int n_time, const float *W, const double *u,
+                 const double *M, const double *q, const double *chi);
+
+/* ------------------------------------------------------------------ analysis */
+
+/* Node geometry (exmarg/search/pe.py:58-84), distance-prior weights
+ * (pe.py:260-286 and :321-327, computed on the device in float64) and cell
+ * weights (pe.py:338-343) for the current store and bank.  prior
+ * EXM_PRIOR_VOLUME, or EXM_PRIOR_TABULATED with the density (lny, p_lny) of
+ * n_dens points ('madau-dickinson', exmarg/priors.py:31-38).  Fails with
+ * EXM_ERR_ARG and the reference's message when a template reaches fewer than
+ * two nodes (pe.py:324-325). */
+EXM_API int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double *lny, const double *p_lny, int n_dens);
+
+/* pe_intrinsic on n_seg segments (exmarg/search/pe.py:289-346): d_H, d_L
+ * (n_seg, nfreq) complex128 (interleaved), sig2_H, sig2_L (nfreq) float64,
+ * seeds (n_seg) the random-draw seed of each segment (seed + row),
+ * n_loud / n_random as gather.select_times (n_loud = 0: every arrival time).
+ * Outputs ln_lambda (n_seg, nm) and ln_b (n_seg) float64 on the host. */
+EXM_API int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const double *d_L, const double *sig2_H,
+                     const double *sig2_L, const int64_t *seeds, int n_loud, int n_random, double *ln_lambda,
+                     double *ln_b);
+
+/* ------------------------------------------------------------------ stages (tests, gather-level drop-in) */
+
+/* Matched filter of one segment (exmarg/search/bank.py:56-78, MassBank.trajectories):
+ * the result stays on the device for the next stages; traj_out, if not NULL,
+ * receives float32 (4, nm, n_time) = lqH, phH, lqL, phL. */
+EXM_API int exm_filter(exm_ctx *ctx, const double *d_H, const double *d_L, const double *sig2_H, const double *sig2_L,
+               float *traj_out);
+
+/* Upload trajectories (4, nm, n_time) float32 = lqH, phH, lqL, phL from the host,
+ * in place of exm_filter. */
+EXM_API int exm_set_trajectories(exm_ctx *ctx, const float *traj);
+
+/* Time selection of the current trajectories (exmarg/search/gather.py:374-420,
+ * select_times), with the numpy PCG64 draw of np.random.default_rng(seed)
+ * reproduced on the device.  sel_out (nm, n_loud + n_random) int32 and lw_out
+ * float32, if not NULL, receive the result. */
+EXM_API int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_random, int32_t *sel_out, float *lw_out);
+
+/* Upload a time selection (nm, nwalk) from the host in place of exm_select_times
+ * (nwalk = 0: every arrival time). */
+EXM_API int exm_set_times(exm_ctx *ctx, int nwalk, const int32_t *sel, const float *lw);
+
+/* The gather contract of exmarg/search/gather.py:114-140 / :340-371
+ * (gather_cpu / gather_gpu) on the current trajectories and times: nsel
+ * (template, slot) rows, mass_ids (nsel), lna and tab_ids (nsel, ns); out
+ * (ns, nsel) float64 ln Lambda.  Arithmetic in float64 like the reference CPU
+ * path. */
+EXM_API int exm_gather(exm_ctx *ctx, int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,
+               double *out);
+
+/* Node values of the current segment (exmarg/search/pe.py:168-200,
+ * _node_values): lamN_out (n_nodes + 1, nm) float64, -inf where a template does
+ * not reach a node; row n_nodes the boundary point.  Uses the plane-staged gather. */
+EXM_API int exm_node_values(exm_ctx *ctx, double *lamN_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
