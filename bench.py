@@ -1,0 +1,316 @@
+"""Benchmark of the Eq. (C7) path (exmarg pe_intrinsic) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one step = one segment analysed end to end through the public API):
+2048-template TaylorF2 bank (chirp mass 10-40, q 0.25-1, chi_eff -0.5..0.5), 53
+signal-power nodes of seeded synthetic float32 tables at the production shape
+(87 lags x 49 phase planes x 200 beta x 219 Delta, 39.8 GB, resident in HBM), 8 s
+H1+L1 segments (20-512 Hz, n_time = 32768) of coloured Gaussian noise with one
+injected TaylorF2 signal (chirp mass 25, q 0.8, chi_eff 0.1, network SNR 15), volume
+prior, n_loud = n_random = 1024.  The tables (39.8 GB) are far larger than the L2
+(126 MB), so no flush is needed between steps.
+
+Under torchrun (N > 1) every rank is an independent replica on its own GPU with its
+own segments (weak scaling); ranks meet only in host-side barriers and the max of
+their device times (gloo).  --impl reference runs the CPU restatement of the
+reference's path (oracle/, float64 gather over the host cores) on rank 0 only.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "segments/s at |dlnB|<=1e-5 (2048 templ, 53 nodes); p50/p99 latency; gather GB/s"
+N_TEMPLATES, T_SEG, FMAX = 2048, 8.0, 512.0
+N_LOUD = N_RANDOM = 1024
+TABLE_SEED, BANK_SEED, SEG_SEED = 2026, 11, 50000
+
+
+def workload_config(args=None):
+    if args is not None and (args.templates != N_TEMPLATES or args.nodes != 53):
+        return {"workload": "reduced profiling case: %d templates, %d nodes (else as the full workload)"
+                            % (args.templates, args.nodes), "templates": args.templates, "nodes": args.nodes,
+                "segment_s": T_SEG, "n_time": 32768, "table_dtype": "f32"}
+    return {"workload": "pe_intrinsic, 1 segment per call: 2048-template TaylorF2 bank, 53 nodes of seeded f32 "
+                        "tables 87x49x200x219 (39.8 GB, resident), 8 s H1+L1 segment 20-512 Hz (n_time 32768), "
+                        "SNR-15 injection, n_loud=n_random=1024, volume prior",
+            "templates": N_TEMPLATES, "nodes": 53, "segment_s": T_SEG, "n_time": 32768,
+            "table_dtype": "f32", "l2": "inputs larger than L2 (39.8 GB tables vs 126 MB)"}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_inputs(n_seg, rank, n_templates=N_TEMPLATES, n_nodes=53):
+    from exmarg_b200 import synth
+    spec = synth.TableSpec()
+    s_nodes = synth.S_NODES_PROD
+    if n_nodes < s_nodes.size:            # a reduced case keeps nodes every template reaches
+        s_nodes = s_nodes[30:30 + n_nodes]
+    seg = synth.make_segments(n_seg, SEG_SEED + 100000 * rank, T=T_SEG, fmax=FMAX, snr=15.0, mc=25.0, q=0.8,
+                              chi=0.1)
+    rows = synth.make_bank(n_templates, BANK_SEED)
+    return spec, s_nodes, seg, rows
+
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU during the timed region"""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [s for s, p in zip(sm, power) if p > 200.0] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per plane-gather launch of this workload, from the committed ncu summary"""
+    path = os.path.join(ROOT, "profiles", "k_gather_planes_prod.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+# ----------------------------------------------------------------------------- CPU baseline (oracle port)
+
+def cpu_sample(seg, rows, W, u, lo, n_time, store, n_templates, e=0):
+    """the CPU restatement of the reference path (oracle) on a template sample of one segment:
+    (seconds, sampled template ids, their ln_lambda)"""
+    from oracle import restate
+    rng = np.random.default_rng(7)
+    idx = np.sort(rng.choice(rows.shape[0], min(n_templates, rows.shape[0]), replace=False))
+    s1 = restate.read_segments(seg, rows=[e])
+    t0 = time.perf_counter()
+    o = restate.pe_intrinsic(s1, W[idx], u[idx], rows[idx, 0], rows[idx, 1], rows[idx, 2], lo, n_time, store,
+                             n_loud=N_LOUD, n_random=N_RANDOM, seed=0, precision="ref", bank_rows=idx,
+                             n_bank=rows.shape[0])
+    return time.perf_counter() - t0, idx, o["ln_lambda"][0]
+
+
+def host_store(spec, s_nodes):
+    from exmarg_b200 import synth
+    from oracle import restate
+    tables = restate.gen_tables(spec, s_nodes, TABLE_SEED)
+    return synth.MemoryStore(spec, s_nodes, TABLE_SEED, tables=tables)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from exmarg_b200 import bank as bank_mod
+    from oracle import restate
+    spec, s_nodes, seg, rows = make_inputs(args.warmup + args.steps, 0, args.templates, args.nodes)
+    store = host_store(spec, s_nodes)
+    b = bank_mod.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg, "b200")
+    n_t = min(args.ref_templates, rows.shape[0])
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, _, _ = cpu_sample(seg, rows, b.W, b.u, b.lo, b.n_time, store, n_t, e=i)
+        if i >= args.warmup:
+            times.append(t)
+    frac = n_t / float(rows.shape[0])
+    value = args.steps * frac / sum(times)
+    cores = restate.num_threads()
+    sample = "%d of %d templates of each 8 s segment (all %d nodes, 87 lags, 2048 walked times), " \
+             "float64 C gather over %d host threads" % (n_t, rows.shape[0], len(s_nodes), cores)
+    line = {"metric": METRIC, "value": value, "unit": "segments/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sum(times) / args.steps / frac,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": value, "unit": "segments/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "segments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- B200 arm
+
+def run_b200(args):
+    rank, world, local = dist_env()
+    import exmarg_b200 as eb
+    from exmarg_b200 import synth, _lib
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    n_seg = args.warmup + args.steps
+    spec, s_nodes, seg, rows = make_inputs(n_seg, rank, args.templates, args.nodes)
+    ctx = eb.context(local)
+    bank = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg, "b200", device_index=local)
+    # the store: every node generated on the device (no 40 GB host copy on the measured path)
+    M, P, Q, S = spec.factors(s_nodes)
+    store = synth.MemoryStore(spec, s_nodes, TABLE_SEED, tables=[None] * len(s_nodes))
+    store.generator = (M, P, Q, S, TABLE_SEED)
+    eb.prepare(bank, store, "volume", 0.1267)
+
+    for i in range(args.warmup):
+        eb.pe_intrinsic(seg, bank, store, rows=[i])
+    ctx.timing(True)
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    lat = []
+    res = []
+    t0 = time.perf_counter()
+    for i in range(args.warmup, n_seg):
+        a = time.perf_counter()
+        r = eb.pe_intrinsic(seg, bank, store, rows=[i])
+        lat.append(time.perf_counter() - a)
+        res.append(r)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    tm = ctx.timing(False)
+    dev_s = tm["total_ms"] / 1000.0
+    if pg:
+        import torch
+        t = torch.tensor([dev_s, wall], dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_s, wall = float(t[0]), float(t[1])
+        pg.barrier()
+    total = args.steps * world
+    value = total / dev_s
+    e2e = total / wall
+    nf = bank.W.shape[1]
+    launches = tm["gather_launches"]
+    g_ms = tm["gather_ms"] / max(launches, 1)
+    bytes_per_launch = (32.0 * tm["node_taps"] + 16.0 * tm["tlw_taps"]) / max(launches, 1)
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_per_launch / (g_ms / 1000.0) / 1e9
+    traffic = profiled_traffic()
+    line = {"metric": METRIC, "value": value, "unit": "segments/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
+            "e2e": {"value": e2e, "unit": "segments/s", "h2d_bytes_per_step": 6 * nf * 8,
+                    "d2h_bytes_per_step": rows.shape[0] * 8 + 8 + 4,
+                    "latency_ms_p50": 1000.0 * float(np.percentile(lat, 50)),
+                    "latency_ms_p99": 1000.0 * float(np.percentile(lat, 99))},
+            "gpu_launches": int(tm["launches"]),
+            "stages_ms_per_step": {k: tm[k] / args.steps for k in ("filter_ms", "select_ms", "taps_ms", "gather_ms",
+                                                                    "epilogue_ms")},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "kernel": "k_gather_planes", "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": g_ms,
+                         "node_taps_per_launch": tm["node_taps"] / max(launches, 1),
+                         "dram_gbs": (traffic / (g_ms / 1000.0) / 1e9) if traffic else None},
+            "gather_gbs_logical": achieved, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # CPU baseline and parity: the oracle on a template sample of the first timed segment
+        store_h = host_store(spec, s_nodes)
+        n_t = min(args.cpu_templates, rows.shape[0])
+        t_cpu, idx, lnl_cpu = cpu_sample(seg, rows, bank.W, bank.u, bank.lo, bank.n_time, store_h, n_t,
+                                         e=args.warmup)
+        from oracle import restate
+        frac = n_t / float(rows.shape[0])
+        lnl_gpu = res[0]["ln_lambda"][0][idx]
+        cell = restate.cell_weights(rows[idx, 0], rows[idx, 1], rows[idx, 2])
+        line["cpu_baseline"] = {"value": frac / t_cpu, "unit": "segments/s", "cores": restate.num_threads(),
+                                "kind": "port",
+                                "sample": "%d of %d templates of one segment (all 53 nodes, 87 lags, 2048 walked "
+                                          "times), float64 C gather, %.1f s" % (n_t, N_TEMPLATES, t_cpu)}
+        line["parity"] = {"templates": n_t, "max_abs_dlnlambda": float(np.abs(lnl_gpu - lnl_cpu).max()),
+                          "sample_dlnB": float(abs(restate.log_mean(lnl_gpu, cell) - restate.log_mean(lnl_cpu, cell)))}
+        del store_h
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-templates", type=int, default=128)
+    ap.add_argument("--ref-templates", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--templates", type=int, default=N_TEMPLATES, help="bank size (reduced profiling cases)")
+    ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

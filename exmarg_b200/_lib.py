@@ -18,7 +18,7 @@ DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_ctx_timing", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values")
@@ -41,10 +41,12 @@ def load():
     P, I, D, Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
     sig = {
         "exm_version": ([], I),
+        "exm_rng_integers": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int64, P], I),
         "exm_ctx_create": ([I, Z, ctypes.POINTER(P)], I),
         "exm_ctx_destroy": ([P], None),
         "exm_last_error": ([P], ctypes.c_char_p),
         "exm_ctx_bytes": ([P], Z),
+        "exm_ctx_timing": ([P, I, P], I),
         "exm_store_init": ([P, I, I, I, I, I, I, P, D, D, D, D], I),
         "exm_store_set_node": ([P, I, D, D, D, P], I),
         "exm_store_generate_node": ([P, I, D, D, D, P, P, P, ctypes.c_float, ctypes.c_uint32], I),
@@ -65,6 +67,15 @@ def load():
         f.restype = res
     _lib = lib
     return lib
+
+
+def rng_integers(seed, high, count):
+    """np.random.default_rng(seed).integers(0, high, count), by the library's host PCG64 code"""
+    out = np.empty(int(count), np.int64)
+    rc = load().exm_rng_integers(int(seed), int(high), int(count), _p(out))
+    if rc != EXM_OK:
+        _raise(rc, "bad rng arguments")
+    return out
 
 
 def _raise(code, msg):
@@ -108,6 +119,15 @@ class Context:
     @property
     def bytes(self):
         return int(self.lib.exm_ctx_bytes(self.h))
+
+    def timing(self, enable=True):
+        """stage times accumulated since the previous call (CUDA events on the context's stream),
+        then reset; enable turns timing on or off for the following calls"""
+        out = np.zeros(16, np.float64)
+        self._check(self.lib.exm_ctx_timing(self.h, 1 if enable else 0, _p(out)))
+        keys = ("total_ms", "filter_ms", "select_ms", "taps_ms", "gather_ms", "epilogue_ms", "gather_launches",
+                "node_taps", "tlw_taps", "segments", "launches", "slow_taps", "boundary_taps")
+        return dict(zip(keys, out[:len(keys)]))
 
     # store ------------------------------------------------------------
     def store_init(self, n_nodes, shape, tau_idx, beta0, dbeta, delta0, ddelta, dtype=DTYPE_F32):

@@ -57,6 +57,7 @@ class MassBank:
         self.n_time = 8 * int(self.nu.max())
         if W is None:
             prof = profile or default_profile()
+            sig2_H = np.asarray(seg["sig2_H"] if "sig2_H" in seg else seg["sig2"], float)
             W = np.empty((self.M.size, self.nu.size), np.complex64)
             u = np.empty(self.M.size)
             for i in range(self.M.size):
@@ -69,7 +70,7 @@ class MassBank:
                 psi0 = np.zeros(self.nu.size)
                 psi0[j] = p0
                 W[i] = a * np.exp(1j * psi0)
-                u[i] = float((a ** 2 / seg["sig2_H"]).sum())
+                u[i] = float((a ** 2 / sig2_H).sum())
         self.W = np.ascontiguousarray(W, np.complex64)
         self.u = np.asarray(u, float)
         self.device_index = device_index

@@ -81,6 +81,40 @@ void exm_fft_plan(exm_ctx *ctx, int batch)
     ctx->plan_n = ctx->nt;
 }
 
+// ------------------------------------------------------------------ stage timers
+
+int exm_tim_begin(exm_ctx *ctx, int stage)
+{
+    if (!ctx->tim_on) return -1;
+    if (ctx->ev_used == ctx->ev_pool.size()) {
+        std::pair<cudaEvent_t, cudaEvent_t> e;
+        EXM_CUDA(cudaEventCreate(&e.first));
+        EXM_CUDA(cudaEventCreate(&e.second));
+        ctx->ev_pool.push_back(e);
+    }
+    const int h = (int)ctx->ev_used++;
+    EXM_CUDA(cudaEventRecord(ctx->ev_pool[h].first, ctx->stream));
+    ctx->ev_pending.push_back({stage, h});
+    return h;
+}
+
+void exm_tim_end(exm_ctx *ctx, int h)
+{
+    if (h < 0) return;
+    EXM_CUDA(cudaEventRecord(ctx->ev_pool[h].second, ctx->stream));
+}
+
+void exm_tim_collect(exm_ctx *ctx)
+{
+    for (auto &pe : ctx->ev_pending) {
+        float ms = 0.f;
+        EXM_CUDA(cudaEventElapsedTime(&ms, ctx->ev_pool[pe.second].first, ctx->ev_pool[pe.second].second));
+        ctx->tacc[pe.first] += ms;
+    }
+    ctx->ev_pending.clear();
+    ctx->ev_used = 0;
+}
+
 // ------------------------------------------------------------------ api plumbing
 
 #define API_BEGIN(ctx)                                                                                             \
@@ -105,7 +139,62 @@ void exm_fft_plan(exm_ctx *ctx, int batch)
         if (!(cond)) EXM_THROW(code, msg);                                                                         \
     } while (0)
 
+extern "C" int exm_ctx_timing(exm_ctx *ctx, int enable, double *out)
+{
+    API_BEGIN(ctx)
+    if (out) {
+        unsigned long long st[4] = {0, 0, 0, 0};
+        if (ctx->d_stats.p) {
+            EXM_CUDA(cudaMemcpy(st, ctx->d_stats.p, sizeof(st), cudaMemcpyDeviceToHost));
+            EXM_CUDA(cudaMemset(ctx->d_stats.p, 0, sizeof(st)));
+        }
+        out[11] = (double)st[0];
+        out[12] = (double)st[1];
+        for (int i = 0; i < 6; ++i) out[i] = ctx->tacc[i];
+        out[6] = (double)ctx->gather_launches;
+        out[7] = ctx->node_taps;
+        out[8] = ctx->tlw;
+        out[9] = ctx->segments;
+        out[10] = (double)ctx->launches;
+    }
+    for (double &t : ctx->tacc) t = 0.0;
+    ctx->node_taps = ctx->tlw = ctx->segments = 0;
+    ctx->gather_launches = ctx->launches = 0;
+    ctx->tim_on = enable != 0;
+    API_END(ctx)
+}
+
 extern "C" int exm_version(void) { return 10000; }
+
+extern "C" int exm_rng_integers(uint64_t seed, uint32_t high, int64_t count, int64_t *out)
+{
+    if (high < 1 || count < 0 || (count > 0 && !out)) return EXM_ERR_ARG;
+    exm_pcg g = exm_pcg_from_seed(seed);
+    const uint32_t rng = high - 1;
+    if (rng == 0) {
+        for (int64_t i = 0; i < count; ++i) out[i] = 0;
+        return EXM_OK;
+    }
+    const uint32_t thr = (uint32_t)((1ull << 32) % high);
+    uint64_t buf = 0;
+    bool have = false;
+    for (int64_t i = 0; i < count;) {
+        uint32_t x;
+        if (have) {
+            x = (uint32_t)(buf >> 32);
+            have = false;
+        } else {
+            exm_pcg_step(g);
+            buf = exm_pcg_output(g.state);
+            x = (uint32_t)buf;
+            have = true;
+        }
+        const uint64_t m = (uint64_t)x * high;
+        if ((uint32_t)m < thr) continue;
+        out[i++] = (int64_t)(m >> 32);
+    }
+    return EXM_OK;
+}
 
 extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
 {
@@ -142,8 +231,12 @@ extern "C" void exm_ctx_destroy(exm_ctx *ctx)
     cudaStreamSynchronize(ctx->stream);
     if (ctx->plan) cufftDestroy(ctx->plan);
     free_slot(ctx, ctx->slot);
+    for (auto &e : ctx->ev_pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
     dbuf *all[] = {&ctx->T, &ctx->d_tau, &ctx->d_W, &ctx->d_bhat_off, &ctx->d_bnode, &ctx->d_cb, &ctx->d_lnW,
-                   &ctx->d_cell, &ctx->d_mlo, &ctx->d_mhi, &ctx->d_order, &ctx->d_cki, &ctx->d_ckd, &ctx->fftwork};
+                   &ctx->d_cell, &ctx->d_mlo, &ctx->d_mhi, &ctx->d_order, &ctx->d_cki, &ctx->d_ckd, &ctx->fftwork, &ctx->d_stats};
     for (dbuf *b : all) exm_free(ctx, *b);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -193,6 +286,8 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
     exm_ensure(ctx, ctx->d_tau, sizeof(int) * ntau);
     EXM_CUDA(cudaMemcpy(ctx->d_tau.p, t32.data(), sizeof(int) * ntau, cudaMemcpyHostToDevice));
     exm_make_tmap(ctx);
+    exm_ensure(ctx, ctx->d_stats, 4 * sizeof(unsigned long long));
+    EXM_CUDA(cudaMemsetAsync(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long), ctx->stream));
     EXM_CUDA(cudaStreamSynchronize(ctx->stream));
     API_END(ctx)
 }
@@ -514,21 +609,42 @@ static void check_dev_err(exm_ctx *ctx, exm_slot &sl)
 // everything of one segment from the staged input to lnl / lnb on the device
 static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs, uint64_t seed)
 {
+    const int tt = exm_tim_begin(ctx, 0);
     EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
-    if (rs.K > 0) exm_run_pcg(ctx, sl, seed, rs.K, rs.S);
+    if (rs.K > 0) {
+        const int h = exm_tim_begin(ctx, 2);
+        exm_run_pcg(ctx, sl, seed, rs.K, rs.S);
+        exm_tim_end(ctx, h);
+    }
     for (int m_base = 0; m_base < ctx->nm; m_base += rs.nmc_max) {
         const int nmc = std::min(rs.nmc_max, ctx->nm - m_base);
+        int h = exm_tim_begin(ctx, 1);
         exm_run_filter(ctx, sl, (const float2 *)ctx->d_W.p + (size_t)m_base * ctx->nfreq, nmc);
-        if (rs.K > 0) exm_run_topk(ctx, sl, nmc, (const int *)ctx->d_order.p + m_base, rs.K, rs.S);
+        exm_tim_end(ctx, h);
+        if (rs.K > 0) {
+            h = exm_tim_begin(ctx, 2);
+            exm_run_topk(ctx, sl, nmc, (const int *)ctx->d_order.p + m_base, rs.K, rs.S);
+            exm_tim_end(ctx, h);
+        }
         ChunkInfo ci{m_base, nmc, rs.nwalk, rs.use_sel, rs.lw};
         for (int r0 = 0; r0 < ctx->ntau; r0 += rs.rc) {
             const int rc = std::min(rs.rc, ctx->ntau - r0);
+            h = exm_tim_begin(ctx, 3);
             exm_run_taps(ctx, sl, ci, r0, rc, r0 == 0);
+            exm_tim_end(ctx, h);
+            h = exm_tim_begin(ctx, 4);
             exm_run_gather_planes(ctx, sl, ci, r0, rc);
+            exm_tim_end(ctx, h);
         }
+        h = exm_tim_begin(ctx, 5);
         exm_run_node_lse(ctx, sl, m_base, nmc);
+        exm_tim_end(ctx, h);
     }
+    const int h = exm_tim_begin(ctx, 5);
     exm_run_lnb(ctx, sl);
+    exm_tim_end(ctx, h);
+    exm_tim_end(ctx, tt);
+    ctx->segments += 1;
 }
 
 extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const double *d_L, const double *sig2_H,
@@ -552,6 +668,7 @@ extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, cons
         EXM_CUDA(cudaMemcpyAsync(lnl.data(), sl.lnl.p, sizeof(double) * ctx->nm, cudaMemcpyDeviceToHost, ctx->stream));
         EXM_CUDA(cudaMemcpyAsync(ln_b + e, sl.lnb.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         check_dev_err(ctx, sl);
+        exm_tim_collect(ctx);
         for (int i = 0; i < ctx->nm; ++i) ln_lambda[(size_t)e * ctx->nm + ctx->order[i]] = lnl[i];
     }
     ctx->traj_ok = ctx->times_ok = false;

@@ -115,11 +115,21 @@ struct exm_ctx {
     std::vector<double> ck;           // (ln s_k - beta0) / dbeta
     dbuf d_cki;                       // int32 [EXM_MAX_NODES]: floor(ck)
     dbuf d_ckd;                       // double [EXM_MAX_NODES]: ck
+    dbuf d_stats;                     // uint64 [4]: gather counters (slow-path taps, boundary taps)
 
     // cuFFT
     cufftHandle plan = 0;
     int plan_batch = 0, plan_n = 0;
     dbuf fftwork;
+
+    // CUDA-event timing of the pipeline stages on the context's stream
+    bool tim_on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    std::vector<std::pair<int, int>> ev_pending;   // (stage, pool index)
+    size_t ev_used = 0;
+    double tacc[8] = {0};        // ms per stage: 0 total, 1 filter, 2 select, 3 taps, 4 gather, 5 epilogue
+    double node_taps = 0, tlw = 0, segments = 0;
+    long long gather_launches = 0, launches = 0;
 
     // current segment state for the stage entry points
     exm_slot slot;
@@ -128,6 +138,11 @@ struct exm_ctx {
     float cur_lw = 0.f;
     std::vector<exm_slot> slots;
 };
+
+// stage timers (no-ops unless timing is on): begin returns a handle for end
+int exm_tim_begin(exm_ctx *ctx, int stage);
+void exm_tim_end(exm_ctx *ctx, int h);
+void exm_tim_collect(exm_ctx *ctx);   // after a stream synchronisation
 
 // allocation with budget accounting
 void exm_alloc(exm_ctx *ctx, dbuf &b, size_t bytes);

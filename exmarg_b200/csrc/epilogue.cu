@@ -157,6 +157,7 @@ void exm_run_node_lse(exm_ctx *ctx, exm_slot &sl, int m_base, int nmc)
         (const double *)sl.part.p, (const double *)ctx->d_lnW.p, (const int *)ctx->d_mlo.p, (const int *)ctx->d_mhi.p,
         (const int *)ctx->d_bnode.p, ctx->nn, ctx->ntau, ctx->nm, m_base, nmc, ctx->nt, (double *)sl.lnl.p, nullptr);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 1;
 }
 
 void exm_run_node_values(exm_ctx *ctx, exm_slot &sl, double *d_lamN)
@@ -172,6 +173,7 @@ void exm_run_lnb(exm_ctx *ctx, exm_slot &sl)
     k_lnb<<<1, 1024, 0, ctx->stream>>>((const double *)sl.lnl.p, (const double *)ctx->d_cell.p, ctx->nm,
                                       (double *)sl.lnb.p);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 1;
 }
 
 void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,

@@ -65,4 +65,5 @@ void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm)
     EXM_CUFFT(cufftExecC2C(ctx->plan, (cufftComplex *)traj, (cufftComplex *)traj, CUFFT_FORWARD));
     k_polar<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(traj, total);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 3;
 }

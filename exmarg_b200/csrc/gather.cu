@@ -33,6 +33,7 @@ struct PlaneArgs {
     const double *boff, *cb, *ckd;
     double *part;
     unsigned *err;
+    unsigned long long *stats;   // [0] slow-path taps, [1] boundary taps (may be null)
     long long tstride, per_lag;
     int nn, ntau, nphif, nb, nd, ndp, nt, nmc, m_base, nm_total, r0;
     float lw;
@@ -236,6 +237,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         if (!ok) continue;
         const float *s0 = win + (p % 3) * SLOT_FLOATS, *s1 = win + ((p + 1) % 3) * SLOT_FLOATS;
         const int beg = offr[p * (a.nmc + 1) + ia], end = offr[p * (a.nmc + 1) + ibd];
+        unsigned n_slow = 0, n_bnd = 0;
         for (int j0 = beg; j0 < end; j0 += 32) {
             const int j = j0 + lane;
             const bool act = j < end;
@@ -262,6 +264,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
                 const int rb = b0 - R0, rd = d0 - C0;
                 const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
                                   b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf > 0.999999f);
+                n_slow += !fast;
                 if (fast) {
                     interp_window(s0, s1, rb * EXM_WD + rd, fbf, fd, w, vB, vE);
                     vE += lwv;
@@ -282,6 +285,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             float cB = -1e30f, cE = 0.f, cS = 0.f;
             if (__any_sync(0xffffffffu, bs >= 0)) {
                 if (bs >= 0) {
+                    ++n_bnd;
                     const float sfr = fb + bcf[bs];
                     const int cy = sfr >= 1.f;
                     const float fbf = cy ? sfr - 1.f : sfr;
@@ -321,6 +325,13 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
                 aB[tr] = B;
                 aE[tr] = E;
                 aS[tr] = S;
+            }
+        }
+        if (a.stats) {
+            const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);
+            if (lane == 0 && (sl_ | bd_)) {
+                atomicAdd(&a.stats[0], (unsigned long long)sl_);
+                atomicAdd(&a.stats[1], (unsigned long long)bd_);
             }
         }
     }
@@ -371,6 +382,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.ckd = (const double *)ctx->d_ckd.p;
     a.part = (double *)sl.part.p;
     a.err = (unsigned *)sl.dev_err.p;
+    a.stats = (unsigned long long *)ctx->d_stats.p;
     a.tstride = (long long)ctx->tstride;
     a.per_lag = (long long)ci.nmc * ci.nwalk;
     a.nn = ctx->nn;
@@ -406,6 +418,17 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     dim3 grid(rc * ctx->nn, (maxn + EXM_TCH - 1) / EXM_TCH);
     k_gather_planes<GATHER_NW><<<grid, GATHER_NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
     EXM_CUDA(cudaGetLastError());
+    // algorithmic work of this launch: one node-tap per (template slot, lag, walked time)
+    double slots = 0;
+    for (int k = 0; k < ctx->nn; ++k) {
+        const int lo = std::max(ctx->mlo[k], ci.m_base), hi = std::min(ctx->mhi[k], ci.m_base + ci.nmc);
+        slots += std::max(0, hi - lo);
+    }
+    for (int i = ci.m_base; i < ci.m_base + ci.nmc; ++i) slots += ctx->bnode[i] >= 0;
+    ctx->node_taps += slots * rc * ci.nwalk;
+    ctx->tlw += (double)ci.nmc * rc * ci.nwalk;
+    ctx->gather_launches += 1;
+    ctx->launches += 1;
 }
 
 // ------------------------------------------------------------------ the general gather contract, float64

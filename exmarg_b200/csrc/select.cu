@@ -306,6 +306,7 @@ void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S)
         raw, rej);
     k_pcg_compact<<<(unsigned)((n_out + 255) / 256), 256, 0, ctx->stream>>>(raw, rej, n_out, (int32_t *)sl.picks.p);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 2;
 }
 
 // scores, top-K, drawn rest times and the sorted merge for the nmc templates of a chunk
@@ -334,4 +335,5 @@ void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk,
     k_topk<<<nmc, 1024, smem_t, ctx->stream>>>((const uint32_t *)sl.keys.p, (const int32_t *)sl.picks.p,
                                                d_order_chunk, nt, K, S, Sp, (int32_t *)sl.sel.p);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 2;
 }

@@ -248,4 +248,5 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           (int *)sl.win.p);
     EXM_CUDA(cudaGetLastError());
+    ctx->launches += 4;
 }

@@ -102,10 +102,10 @@ def upload_store(store, ctx):
     token = id(store)
     if ctx.store_token == token:
         return
-    shape = tuple(np.asarray(store.tables[0]).shape)
+    gen = getattr(store, "generator", None)
+    shape = tuple(store.spec.shape) if gen is not None else tuple(np.asarray(store.tables[0]).shape)
     beta0, dbeta, delta0, ddelta = store_grid(store)
     ctx.store_init(len(store.tables), shape, store.tau_idx, beta0, dbeta, delta0, ddelta)
-    gen = getattr(store, "generator", None)
     for k, T in enumerate(store.tables):
         if gen is not None and T is None:
             M, P, Q, S, seed = gen

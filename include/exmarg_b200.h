@@ -59,6 +59,21 @@ EXM_API const char *exm_last_error(const exm_ctx *ctx);
 /* Bytes of device memory the context holds now. */
 EXM_API size_t exm_ctx_bytes(const exm_ctx *ctx);
 
+/* numpy's np.random.default_rng(seed).integers(0, high, count) computed on the
+ * host with the same PCG64 / SeedSequence / Lemire code the selection kernel runs
+ * on the device (exmarg/search/gather.py:397).  No GPU needed. */
+EXM_API int exm_rng_integers(uint64_t seed, uint32_t high, int64_t count, int64_t *out);
+
+/* Stage timing with CUDA events on the context's stream.  Returns (if out is not
+ * NULL) what was accumulated since the previous call, then resets and turns timing
+ * on (enable = 1) or off: out[0] device ms of whole segments (inputs already on the
+ * device), out[1..5] ms of filter, selection, tap build, plane gather, epilogue,
+ * out[6] plane-gather launches, out[7] node-taps, out[8] (template, lag, time)
+ * taps, out[9] segments, out[10] kernel launches of this library, out[11] taps
+ * that took the exact float64 path, out[12] boundary-point taps.  No reference
+ * counterpart (the reference times with time.time() in its notebooks). */
+EXM_API int exm_ctx_timing(exm_ctx *ctx, int enable, double *out);
+
 /* ------------------------------------------------------------------ store */
 
 /* Declare the store: n_nodes tables of shape (ntau, nphif, nb, nd), stored on the

@@ -1,5 +1,5 @@
-"""ORACLE -- test infrastructure only.  Compiles the C restatement (gather_fp64.c)
-into oracle/_build/liboracle.so with gcc.  No reference source is compiled: the
+"""ORACLE -- test infrastructure only.  Compiles the C restatement (gather_fp64.c) and
+the C table generator (gen_tables.c) into oracle/_build/liboracle.so with gcc.  No reference source is compiled: the
 reference's path is Python + numba, so there is no oracle/_ref."""
 
 import os
@@ -9,12 +9,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_build", "liboracle.so")
 
 
+SOURCES = ("gather_fp64.c", "gen_tables.c")
+
+
 def build(force=False):
-    src = os.path.join(HERE, "gather_fp64.c")
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= os.path.getmtime(src):
+    srcs = [os.path.join(HERE, s) for s in SOURCES]
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(s) for s in srcs):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    subprocess.check_call(["gcc", "-O2", "-fopenmp", "-shared", "-fPIC", "-o", OUT, src, "-lm"])
+    subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-shared", "-fPIC", "-o", OUT] + srcs +
+                          ["-lm"])
     return OUT
 
 

@@ -42,12 +42,29 @@ def _lib():
                                       ctypes.c_int, P, P, ctypes.c_int, P]
         lib.oracle_gather.restype = ctypes.c_int
         lib.oracle_num_threads.restype = ctypes.c_int
+        lib.oracle_gen_node.argtypes = [P, P, P, P, ctypes.c_float, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        lib.oracle_gen_node.restype = None
         _LIB = lib
     return _LIB
 
 
 def num_threads():
     return int(_lib().oracle_num_threads())
+
+
+def gen_tables(spec, s_nodes, seed, factors=None):
+    """every node table of the seeded synthetic store, generated in C over the host cores
+    (bit-identical to exmarg_b200.synth.gen_table_node)"""
+    M, P, Q, S = factors if factors is not None else spec.factors(s_nodes)
+    M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))
+    out = []
+    for k in range(len(s_nodes)):
+        T = np.empty(spec.shape, np.float32)
+        _lib().oracle_gen_node(T.ctypes.data, M.ctypes.data, P.ctypes.data, Q.ctypes.data, float(S[k]), int(seed),
+                               k, spec.ntau, spec.nphif, spec.nb, spec.nd)
+        out.append(T)
+    return out
 
 
 # ----------------------------------------------------------------------------- segments
@@ -95,10 +112,13 @@ def trajectories(W, d, sig2, lo, n_time, precision="fp64"):
 
 # ----------------------------------------------------------------------------- time selection
 
-def select_times(traj, tau_idx, n_loud, n_random, seed):
+def select_times(traj, tau_idx, n_loud, n_random, seed, bank_rows=None, n_bank=None):
     """exmarg/search/gather.py:374-420: the n_loud loudest times by |z_L|^2 + max_tau |z_H(t+tau)|^2,
     plus n_random host-RNG draws from the rest with log weight ln((n_time - n_loud) / n_random);
-    returns (sel int32, lw float32), (n_template, n_loud + n_random), sorted by time."""
+    returns (sel int32, lw float32), (n_template, n_loud + n_random), sorted by time.
+
+    bank_rows / n_bank: the trajectories are rows bank_rows of an n_bank-template bank; the draws
+    are then the rows of the whole bank's (n_bank, n_random) draw, as the reference takes them."""
     K, S = int(n_loud), int(n_random)
     lqH, lqL = traj["lqH"], traj["lqL"]
     nm, nt = lqH.shape
@@ -106,7 +126,10 @@ def select_times(traj, tau_idx, n_loud, n_random, seed):
     lo, hi = int(lags.min()), int(lags.max())
     if not np.array_equal(np.sort(lags), np.arange(lo, hi + 1)):
         raise ValueError("lags are not contiguous")
-    pick = np.random.default_rng(seed).integers(0, nt - K, size=(nm, S))
+    if bank_rows is None:
+        pick = np.random.default_rng(seed).integers(0, nt - K, size=(nm, S))
+    else:
+        pick = np.random.default_rng(seed).integers(0, nt - K, size=(int(n_bank), S))[np.asarray(bank_rows)]
     # the sliding maximum over lags lo..hi (a direct window maximum; ln|z| is monotone in |z|^2)
     mx = np.full_like(lqH, -np.inf)
     for tau in range(lo, hi + 1):
@@ -273,12 +296,15 @@ def node_values(traj, store, geometry, groups, times):
 
 def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0.1267, nodes_per_launch=6,
                  n_loud=1024, n_random=1024, seed=0, precision="fp64", density=None, times=None,
-                 return_parts=False):
+                 return_parts=False, bank_rows=None, n_bank=None):
     """exmarg/search/pe.py:289-346 for the segments of seg (read_segments output).
 
     W (n_template, n_freq) complex template factors, u (n_template,) their powers.
     times: optional list (one per segment) of (sel, lw) to use instead of select_times
     (so that a numerical comparison is made on the same visited times).
+    bank_rows / n_bank: W, u, M, q, chi are rows bank_rows of an n_bank-template bank (a
+    template sample); the random draws are taken as for the whole bank (ln_b is then over
+    the sample only).
     returns dict ln_lambda (n_seg, n_template), ln_b (n_seg,) [, parts]"""
     geometry = node_geometry(store.s, store.alpha_lo, store.alpha_hi, u, ymin)
     yN = geometry[2]
@@ -294,7 +320,7 @@ def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0
         if times is not None:
             tm = times[e]
         elif n_loud > 0:
-            tm = select_times(traj, store.tau_idx, n_loud, n_random, seed + int(seg["rows"][e]))
+            tm = select_times(traj, store.tau_idx, n_loud, n_random, seed + int(seg["rows"][e]), bank_rows, n_bank)
         else:
             tm = None
         lamN = node_values(traj, store, geometry, groups, tm)

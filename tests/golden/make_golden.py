@@ -1,0 +1,94 @@
+"""Golden vectors for the pe_intrinsic path, produced by running the REFERENCE's own CPU
+code (exmarg.search: numpy + numba) in a container where its source tree is present.
+
+    python tests/golden/make_golden.py [reference src dir]
+
+Each fixture holds the inputs (segments, bank rows, W and u, the store geometry and the
+float32 generator factors of its seeded tables) and the reference's outputs (ln_lambda,
+ln_b, the visited times of segment 0, and a gather_cpu result).  The tests regenerate
+the tables from the stored factors (bit-exact, see exmarg_b200.synth) and compare the
+oracle and the B200 path against these outputs; nothing at test time reads the
+reference.
+"""
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from exmarg_b200 import synth  # noqa: E402
+from oracle import refimport  # noqa: E402
+
+CASES = {
+    # BASELINE config 1 shape: 8 s, analysis band 20-256 Hz (lag unit 1/2048 s, lags +-21),
+    # 3 nodes at reduced beta/Delta settings, 64 templates
+    "config1": dict(T=8.0, fmax=256.0, ntau=43, nb=100, nd=109, nodes=(14, 24, 34), n_template=64, n_seg=2,
+                    snr=15.0, n_loud=1024, n_random=1024, seed_seg=100, seed_bank=3, seed_tab=7, prior="volume"),
+    # production lag/table shape (87 lags, 200 x 219), 6 consecutive nodes, 4 s segments
+    "prodshape": dict(T=4.0, fmax=512.0, ntau=87, nb=200, nd=219, nodes=tuple(range(20, 26)), n_template=16,
+                      n_seg=2, snr=(5.0, 30.0), n_loud=256, n_random=256, seed_seg=500, seed_bank=11, seed_tab=19,
+                      prior="volume"),
+    # every arrival time walked (n_loud = 0), the tabulated Madau-Dickinson prior, a noise-only segment
+    "alltimes_md": dict(T=4.0, fmax=256.0, ntau=43, nb=100, nd=109, nodes=(16, 20, 24, 28), n_template=12,
+                        n_seg=2, snr=12.0, noise_only=0.5, n_loud=0, n_random=0, seed_seg=900, seed_bank=5,
+                        seed_tab=23, prior="madau-dickinson"),
+}
+
+
+def make(name, c, search):
+    spec = synth.TableSpec(ntau=c["ntau"], nphif=49, nb=c["nb"], nd=c["nd"])
+    s_nodes = synth.S_NODES_PROD[list(c["nodes"])]
+    store = synth.MemoryStore(spec, s_nodes, c["seed_tab"])
+    seg = synth.make_segments(c["n_seg"], c["seed_seg"], T=c["T"], fmax=c["fmax"], snr=c["snr"],
+                              noise_only=c.get("noise_only", 0.0))
+    rows = synth.make_bank(c["n_template"], c["seed_bank"])
+    bank = search.mass_bank(rows, seg, "cpu")
+    ymin = 0.1267
+    if c["prior"] == "madau-dickinson":
+        import exmarg.priors as pri
+        ymin = float(pri.madau_dickinson_ymin())
+    res = search.pe_intrinsic(seg, bank, store, prior=c["prior"], ymin=ymin, n_loud=c["n_loud"],
+                              n_random=c["n_random"], seed=0)
+    out = dict(d_H=seg["d_H"], d_L=seg["d_L"], f=seg["f"], nu=seg["nu"], sig2=seg["sig2"], T=seg["T"],
+               fmin=seg["fmin"], fmax=seg["fmax"], snr=seg["snr"], bank_rows=rows, W=bank.W, u=bank.u,
+               lo=bank.lo, n_time=bank.n_time, s_nodes=s_nodes, tab_seed=c["seed_tab"], ntau=spec.ntau,
+               nb=spec.nb, nd=spec.nd, ymin=ymin, prior=c["prior"], n_loud=c["n_loud"], n_random=c["n_random"],
+               ln_lambda=res["ln_lambda"], ln_b=res["ln_b"])
+    M, P, Q, S = spec.factors(s_nodes)
+    out.update(fac_M=M, fac_P=P, fac_Q=Q, fac_S=S)
+    if c["prior"] == "madau-dickinson":
+        import exmarg.priors as pri
+        lny, p = pri.distance_density("madau-dickinson")
+        out.update(dens_lny=lny, dens_p=p)
+    # visited times and one gather_cpu call on segment 0 (its trajectories, all nodes of the first group)
+    d = {I: np.asarray(seg["d_" + I][0], complex) for I in "HL"}
+    traj = bank.trajectories(d, {I: np.asarray(seg["sig2"], float) for I in "HL"})
+    if c["n_loud"] > 0:
+        sel, lw = search.gather.select_times(traj, store.tau_idx, c["n_loud"], c["n_random"], 0)
+        out.update(sel0=sel, lw0=lw)
+        times = (sel, lw)
+    else:
+        times = None
+    ns = min(3, s_nodes.size)
+    a = s_nodes[:ns][None, :] / bank.u[:, None]
+    lna = np.log(a)
+    tab = np.tile(np.arange(ns), (bank.u.size, 1))
+    g = search.gather.gather_cpu(traj, dict(T=store.tables[:ns], tau=store.tau_idx, beta=spec.beta,
+                                            delta=spec.delta), np.arange(bank.u.size), lna, tab, times)
+    out.update(gather_lna=lna, gather_tab=tab, gather_out=g)
+    np.savez_compressed(os.path.join(HERE, "%s.npz" % name), **out)
+    print(name, "ln_b", res["ln_b"], "size %.1f MB" % (os.path.getsize(os.path.join(HERE, "%s.npz" % name)) / 1e6))
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
+    search = refimport.import_reference(src)
+    for name, c in CASES.items():
+        make(name, c, search)
+
+
+if __name__ == "__main__":
+    main()
