@@ -38,10 +38,10 @@ TABLE_SEED, BANK_SEED, SEG_SEED = 2026, 11, 50000
 
 
 def workload_config(args=None):
-    if args is not None and (args.templates != N_TEMPLATES or args.nodes != 53):
-        return {"workload": "reduced profiling case: %d templates, %d nodes (else as the full workload)"
-                            % (args.templates, args.nodes), "templates": args.templates, "nodes": args.nodes,
-                "segment_s": T_SEG, "n_time": 32768, "table_dtype": "f32"}
+    if args is not None and (args.templates != N_TEMPLATES or args.nodes != 53 or args.lags != 87):
+        return {"workload": "reduced profiling case: %d templates, %d nodes, %d lags (else as the full workload)"
+                            % (args.templates, args.nodes, args.lags), "templates": args.templates,
+                "nodes": args.nodes, "lags": args.lags, "segment_s": T_SEG, "n_time": 32768, "table_dtype": "f32"}
     return {"workload": "pe_intrinsic, 1 segment per call: 2048-template TaylorF2 bank, 53 nodes of seeded f32 "
                         "tables 87x49x200x219 (39.8 GB, resident), 8 s H1+L1 segment 20-512 Hz (n_time 32768), "
                         "SNR-15 injection, n_loud=n_random=1024, volume prior",
@@ -56,9 +56,9 @@ def dist_env():
     return rank, world, local
 
 
-def make_inputs(n_seg, rank, n_templates=N_TEMPLATES, n_nodes=53):
+def make_inputs(n_seg, rank, n_templates=N_TEMPLATES, n_nodes=53, n_lags=87):
     from exmarg_b200 import synth
-    spec = synth.TableSpec()
+    spec = synth.TableSpec(ntau=n_lags)
     s_nodes = synth.S_NODES_PROD
     if n_nodes < s_nodes.size:            # a reduced case keeps nodes every template reaches
         s_nodes = s_nodes[30:30 + n_nodes]
@@ -172,7 +172,7 @@ def run_reference(args):
         return 0
     from exmarg_b200 import bank as bank_mod
     from oracle import restate
-    spec, s_nodes, seg, rows = make_inputs(args.warmup + args.steps, 0, args.templates, args.nodes)
+    spec, s_nodes, seg, rows = make_inputs(args.warmup + args.steps, 0, args.templates, args.nodes, args.lags)
     store = host_store(spec, s_nodes)
     b = bank_mod.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg, "b200")
     n_t = min(args.ref_templates, rows.shape[0])
@@ -209,7 +209,7 @@ def run_b200(args):
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
         pg = dist
     n_seg = args.warmup + args.steps
-    spec, s_nodes, seg, rows = make_inputs(n_seg, rank, args.templates, args.nodes)
+    spec, s_nodes, seg, rows = make_inputs(n_seg, rank, args.templates, args.nodes, args.lags)
     ctx = eb.context(local)
     bank = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg, "b200", device_index=local)
     # the store: every node generated on the device (no 40 GB host copy on the measured path)
@@ -304,6 +304,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--templates", type=int, default=N_TEMPLATES, help="bank size (reduced profiling cases)")
     ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
+    ap.add_argument("--lags", type=int, default=87, help="table lags (reduced profiling cases; odd)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

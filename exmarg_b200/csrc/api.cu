@@ -56,7 +56,7 @@ void exm_ensure(exm_ctx *ctx, dbuf &b, size_t bytes)
 
 static void free_slot(exm_ctx *ctx, exm_slot &s)
 {
-    dbuf *all[] = {&s.traj, &s.keys, &s.picks, &s.rej, &s.sel, &s.hist, &s.win, &s.cnt,
+    dbuf *all[] = {&s.traj, &s.fft, &s.keys, &s.picks, &s.rej, &s.sel, &s.hist, &s.win, &s.cnt,
                    &s.desc, &s.tside, &s.part, &s.lnl, &s.lnb, &s.dev_err, &s.din};
     for (dbuf *b : all) exm_free(ctx, *b);
     if (s.hostin.p) cudaFreeHost(s.hostin.p);
@@ -73,7 +73,7 @@ void exm_fft_plan(exm_ctx *ctx, int batch)
     EXM_CUFFT(cufftSetAutoAllocation(ctx->plan, 0));
     long long n = ctx->nt;
     size_t ws = 0;
-    EXM_CUFFT(cufftMakePlanMany64(ctx->plan, 1, &n, nullptr, 1, n, nullptr, 1, n, CUFFT_C2C, batch, &ws));
+    EXM_CUFFT(cufftMakePlanMany64(ctx->plan, 1, &n, nullptr, 1, n, nullptr, 1, n, CUFFT_Z2Z, batch, &ws));
     exm_ensure(ctx, ctx->fftwork, ws);
     EXM_CUFFT(cufftSetWorkArea(ctx->plan, ctx->fftwork.p));
     EXM_CUFFT(cufftSetStream(ctx->plan, ctx->stream));
@@ -560,6 +560,7 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
 {
     const size_t nmc = rs.nmc_max, nt = ctx->nt, nf = ctx->nfreq;
     exm_ensure(ctx, sl.traj, 2 * nmc * nt * sizeof(float2));
+    exm_ensure(ctx, sl.fft, 2 * nmc * nt * sizeof(double2));
     const size_t n_draws = rs.K > 0 ? (((size_t)ctx->nm * rs.S + EXM_MAX_REJ + 63) / 64) * 64 : 0;
     exm_ensure(ctx, sl.keys, std::max<size_t>(rs.K > 0 ? nmc * nt : 1, n_draws) * sizeof(uint32_t));
     exm_ensure(ctx, sl.picks, std::max<size_t>(1, (size_t)ctx->nm * rs.S) * sizeof(int32_t));

@@ -35,7 +35,7 @@ struct PlaneArgs {
     unsigned *err;
     unsigned long long *stats;   // [0] slow-path taps, [1] boundary taps (may be null)
     long long tstride, per_lag;
-    int nn, ntau, nphif, nb, nd, ndp, nt, nmc, m_base, nm_total, r0;
+    int nn, ntau, nphif, nb, nd, ndp, nt, nmc, m_base, nm_total, r0, tch, nch;
     float lw;
     double rph, rdb, rdd, offd;
     int cki[EXM_MAX_NODES];
@@ -136,6 +136,136 @@ __device__ __forceinline__ void split_double(double v, float &B, float &E)
     E = (float)(v - (double)B);
 }
 
+// One run of tap descriptors (sorted by template) on the two staged planes of pair p.
+// Each lane takes 4 consecutive taps of a 128-tap chunk and merges equal-template taps in
+// registers; a template that lies inside one lane's taps is merged into its accumulator by
+// that lane, one that spans lanes is combined by a segmented shuffle reduction once per chunk.
+struct RunCtx {
+    const uint4 *descr;
+    const int32_t *tsr;
+    const float *s0, *s1;
+    float *aB, *aE, *aS;        // accumulators of the run's templates, index t - lo
+    const int *bci;             // boundary runs: per-template integer offset (index t - lo)
+    const float *bcf;           //                and fraction
+    const int *bnode;           // boundary runs: which templates have their boundary here
+    int lo, m_base, n, R0, C0, cki, k, r, tau0, nt;
+    float ckf, lw;
+    double offb_node;           // (ln s_k - beta0)/dbeta, regular runs
+};
+
+template <bool BND>
+__device__ __forceinline__ void tap_value(const PlaneArgs &a, const RunCtx &c, uint4 q, int j, int tr, float &vB,
+                                          float &vE, unsigned &n_slow)
+{
+    const int il = (int)(q.w >> 19);
+    const float fb = __uint_as_float(q.x), fd = __uint_as_float(q.y);
+    const float w = __uint_as_float(q.z & 0x7FFFFFFFu);
+    const float lwv = (q.z >> 31) ? c.lw : 0.f;
+    const int d0 = (int)((q.w >> 11) & 0xFFu);
+    const int ibh = ((int)(q.w << 21)) >> 21;
+    const float sfr = fb + (BND ? c.bcf[tr] : c.ckf);
+    const int cy = sfr >= 1.f;
+    const float fbf = cy ? sfr - 1.f : sfr;
+    const int b0 = ibh + (BND ? c.bci[tr] : c.cki) + cy;
+    const int rb = b0 - c.R0, rd = d0 - c.C0;
+    const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
+                      b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf > 0.999999f);
+    if (fast) {
+        interp_window(c.s0, c.s1, rb * EXM_WD + rd, fbf, fd, w, vB, vE);
+    } else {
+        ++n_slow;
+        const int t = c.tsr[j];
+        int i1 = t + c.tau0;
+        if (i1 >= c.nt) i1 -= c.nt;
+        const int gi = il + c.m_base;
+        const double offb = (BND ? a.cb[gi] : c.offb_node) + a.boff[gi];
+        const double v = exm_tap_fp64<float>(a.L[(long long)il * c.nt + t], a.H[(long long)il * c.nt + i1], offb, c.r,
+                                             a.T + (long long)c.k * a.tstride, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
+                                             a.rdd, a.offd);
+        split_double(v, vB, vE);
+    }
+    vE += lwv;
+}
+
+__device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, float E, float S)
+{
+    float b = c.aB[tr], e = c.aE[tr], s = c.aS[tr];
+    lse_merge(b, e, s, B, E, S);
+    c.aB[tr] = b;
+    c.aE[tr] = e;
+    c.aS[tr] = s;
+}
+
+template <bool BND>
+__device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
+{
+    const int lane = threadIdx.x & 31;
+    uint4 qn[4];
+    int jn = beg + 4 * lane;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) qn[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
+    for (int j0 = beg; j0 < end; j0 += 128) {
+        uint4 q[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) q[u] = qn[u];
+        const int jb = j0 + 4 * lane;
+        jn = jb + 128;
+        if (j0 + 128 < end) {   // prefetch the next chunk
+#pragma unroll
+            for (int u = 0; u < 4; ++u) qn[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
+        }
+        int tr[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int t = (jb + u < end) ? (int)(q[u].w >> 19) + c.m_base - c.lo : -1;
+            if (t >= c.n) {   // outside the block's templates: report and skip
+                atomicOr(a.err, EXM_DEVERR_BOUNDS);
+                t = -1;
+            }
+            if (BND && t >= 0 && c.bnode[t + c.lo] != c.k) t = -1;
+            tr[u] = t;
+        }
+        // lane-local merge of the 4 taps; cT is the lane's last template, fT its first closed one
+        int cT = -1, fT = -1;
+        float cB = -1e30f, cE = 0.f, cS = 0.f, fB = -1e30f, fE = 0.f, fS = 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (tr[u] < 0) continue;
+            float vB, vE;
+            tap_value<BND>(a, c, q[u], jb + u, tr[u], vB, vE, n_slow);
+            if (tr[u] == cT) {
+                lse_merge(cB, cE, cS, vB, vE, 1.f);
+            } else {
+                if (cT >= 0) {
+                    if (fT < 0) {
+                        fT = cT;
+                        fB = cB;
+                        fE = cE;
+                        fS = cS;
+                    } else {
+                        acc_merge(c, cT, cB, cE, cS);   // lies inside this lane's taps
+                    }
+                }
+                cT = tr[u];
+                cB = vB;
+                cE = vE;
+                cS = 1.f;
+            }
+        }
+        // the first closed template of lane l + 1 continues lane l's last one, or is lane l + 1's alone
+        const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
+        const float nB = __shfl_down_sync(0xffffffffu, fB, 1);
+        const float nE = __shfl_down_sync(0xffffffffu, fE, 1);
+        const float nS = __shfl_down_sync(0xffffffffu, fS, 1);
+        const int pT = __shfl_up_sync(0xffffffffu, cT, 1);
+        if (lane < 31 && nT >= 0 && nT == cT) lse_merge(cB, cE, cS, nB, nE, nS);
+        if (fT >= 0 && !(lane > 0 && pT == fT)) acc_merge(c, fT, fB, fE, fS);
+        // last templates: runs across consecutive lanes
+        const bool head = seg_reduce(cT >= 0 ? cT : -2 - lane, cB, cE, cS);
+        if (head && cT >= 0) acc_merge(c, cT, cB, cE, cS);
+    }
+}
+
 template <int NW>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
 {
@@ -143,88 +273,85 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     float *win = (float *)smem;
     uint64_t *mbar = (uint64_t *)(smem + 3 * SLOT_BYTES);
     float *aB = (float *)(smem + 3 * SLOT_BYTES + 64);
-    float *aE = aB + EXM_TCH, *aS = aE + EXM_TCH;
-    float *bB = aS + EXM_TCH, *bE = bB + EXM_TCH, *bS = bE + EXM_TCH;
-    float *bcf = bS + EXM_TCH;               // boundary offset, fraction
-    int *bci = (int *)(bcf + EXM_TCH);       // boundary offset, integer part
-    short *bslot = (short *)(bci + EXM_TCH);
-    __shared__ int scan_sh[33];
+    const int tch = a.tch;
+    float *aE = aB + tch, *aS = aE + tch;
+    float *bB = aS + tch, *bE = bB + tch, *bS = bE + tch;
+    float *bcf = bS + tch;
+    int *bci = (int *)(bcf + tch);
 
-    const int k = blockIdx.x % a.nn, rl = blockIdx.x / a.nn, r = a.r0 + rl;
+    // block -> (lag, node, template chunk), lags outermost so the blocks of one lag run together
+    const int c_idx = blockIdx.x % a.nch;
+    const int k = (blockIdx.x / a.nch) % a.nn;
+    const int rl = blockIdx.x / (a.nch * a.nn), r = a.r0 + rl;
     const int lo0 = max(a.mlo[k], a.m_base), hi0 = min(a.mhi[k], a.m_base + a.nmc);
-    const int lo = lo0 + blockIdx.y * EXM_TCH;
-    const int hi = min(hi0, lo + EXM_TCH);
+    const int lo = lo0 + c_idx * tch;
+    const int hi = min(hi0, lo + tch);
     if (lo >= hi) return;
     const int n = hi - lo;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // accumulators and the boundary-slot map (templates whose lowest point is node k)
-    int carry = 0;
-    for (int j0 = 0; j0 < n; j0 += NW * 32) {
-        const int j = j0 + tid;
-        const int isb = (j < n) && a.bnode[lo + j] == k;
-        int v = isb, x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) scan_sh[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int s = lane < NW ? scan_sh[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            if (lane < NW) scan_sh[lane] = s;
-        }
-        __syncthreads();
-        const int excl = carry + x - v + (warp ? scan_sh[warp - 1] : 0);
-        if (j < n) {
-            aB[j] = -1e30f;
-            aE[j] = 0.f;
-            aS[j] = 0.f;
-            bslot[j] = isb ? (short)excl : (short)-1;
-            if (isb) {
-                bB[excl] = -1e30f;
-                bE[excl] = 0.f;
-                bS[excl] = 0.f;
-                const double c = a.cb[lo + j];
-                const double f = floor(c);
-                bci[excl] = (int)f;
-                bcf[excl] = (float)(c - f);
-            }
-        }
-        carry += scan_sh[NW - 1];
-        __syncthreads();
+    // accumulators; the boundary range [blo, bhi) of the templates whose lowest point is node k
+    __shared__ int bl_sh[2];
+    if (tid == 0) {
+        bl_sh[0] = n;
+        bl_sh[1] = 0;
     }
-
+    __syncthreads();
+    for (int j = tid; j < n; j += NW * 32) {
+        aB[j] = -1e30f;
+        aE[j] = 0.f;
+        aS[j] = 0.f;
+        if (a.bnode[lo + j] == k) {
+            bB[j] = -1e30f;
+            bE[j] = 0.f;
+            bS[j] = 0.f;
+            const double cbv = a.cb[lo + j];
+            const double f = floor(cbv);
+            bci[j] = (int)f;
+            bcf[j] = (float)(cbv - f);
+            atomicMin(&bl_sh[0], j);
+            atomicMax(&bl_sh[1], j + 1);
+        }
+    }
     const int C0 = a.win[0], R0 = a.win[1 + k];
-    const int cki = a.cki[k];
-    const float ckf = a.ckf[k];
     if (tid == 0) {
         for (int s = 0; s < 3; ++s) mbar_init(&mbar[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    const int blo = bl_sh[0], bhi = bl_sh[1];
     if (tid == 0) {
         tma_load_plane(&tmap, &mbar[0], win, C0, R0, 0, r, k, SLOT_BYTES);
         tma_load_plane(&tmap, &mbar[1], win + SLOT_FLOATS, C0, R0, 1, r, k, SLOT_BYTES);
     }
     int issued = 2;
 
-    const int wa = lo + (int)((long long)n * warp / NW), wb = lo + (int)((long long)n * (warp + 1) / NW);
-    const int ia = wa - a.m_base, ibd = wb - a.m_base;
+    const int wa = (int)((long long)n * warp / NW), wb = (int)((long long)n * (warp + 1) / NW);   // block-local
     const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
-    const uint4 *descr = a.desc + (long long)rl * a.per_lag;
-    const int32_t *tsr = a.tside + (long long)rl * a.per_lag;
-    const float *Tk = a.T + (long long)k * a.tstride;
     const int nt = a.nt;
-    const int tau0 = ((a.tau[r] % nt) + nt) % nt;
-    const double ckd = a.ckd[k];
+    RunCtx rc;
+    rc.descr = a.desc + (long long)rl * a.per_lag;
+    rc.tsr = a.tside + (long long)rl * a.per_lag;
+    rc.bci = bci - 0;
+    rc.bcf = bcf;
+    rc.bnode = a.bnode;
+    rc.lo = lo;
+    rc.m_base = a.m_base;
+    rc.n = n;
+    rc.R0 = R0;
+    rc.C0 = C0;
+    rc.cki = a.cki[k];
+    rc.ckf = a.ckf[k];
+    rc.k = k;
+    rc.r = r;
+    rc.tau0 = ((a.tau[r] % nt) + nt) % nt;
+    rc.nt = nt;
+    rc.lw = a.lw;
+    rc.offb_node = a.ckd[k];
+    const int ib0 = max(wa, blo), ib1 = min(wb, bhi);   // this warp's boundary templates
+    const int base_i = lo - a.m_base;                    // chunk-local index of template lo
 
+    unsigned n_slow = 0, n_bnd = 0;
     bool ok = mbar_wait(&mbar[0], 0, a.err);
     for (int p = 0; p < EXM_NPAIR; ++p) {
         if (p > 0) __syncthreads();   // every warp is done with plane p - 1: its slot can be refilled
@@ -235,104 +362,27 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         }
         ok = ok && mbar_wait(&mbar[(p + 1) % 3], ((p + 1) / 3) & 1, a.err);
         if (!ok) continue;
-        const float *s0 = win + (p % 3) * SLOT_FLOATS, *s1 = win + ((p + 1) % 3) * SLOT_FLOATS;
-        const int beg = offr[p * (a.nmc + 1) + ia], end = offr[p * (a.nmc + 1) + ibd];
-        unsigned n_slow = 0, n_bnd = 0;
-        for (int j0 = beg; j0 < end; j0 += 32) {
-            const int j = j0 + lane;
-            const bool act = j < end;
-            uint4 q = make_uint4(0u, 0u, 0u, 0u);
-            if (act) q = __ldg(descr + j);
-            const int il = (int)(q.w >> 19);                  // chunk-local template
-            int tr = act ? il + a.m_base - lo : -1;           // template within the block
-            if (act && (unsigned)tr >= (unsigned)n) {         // a descriptor outside the warp's run: report, skip
-                atomicOr(a.err, EXM_DEVERR_BOUNDS);
-                tr = -1;
-            }
-            const bool use = act && tr >= 0;
-            const float fb = __uint_as_float(q.x), fd = __uint_as_float(q.y);
-            const float w = __uint_as_float(q.z & 0x7FFFFFFFu);
-            const float lwv = (q.z >> 31) ? a.lw : 0.f;
-            const int d0 = (int)((q.w >> 11) & 0xFFu);
-            const int ibh = ((int)(q.w << 21)) >> 21;
-            float vB = -1e30f, vE = 0.f, vS = 0.f;
-            if (use) {
-                const float sfr = fb + ckf;
-                const int cy = sfr >= 1.f;
-                const float fbf = cy ? sfr - 1.f : sfr;
-                const int b0 = ibh + cki + cy;
-                const int rb = b0 - R0, rd = d0 - C0;
-                const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
-                                  b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf > 0.999999f);
-                n_slow += !fast;
-                if (fast) {
-                    interp_window(s0, s1, rb * EXM_WD + rd, fbf, fd, w, vB, vE);
-                    vE += lwv;
-                } else {
-                    const int t = tsr[j];
-                    int i1 = t + tau0;
-                    if (i1 >= nt) i1 -= nt;
-                    const double v = exm_tap_fp64<float>(a.L[(long long)il * nt + t], a.H[(long long)il * nt + i1],
-                                                         ckd + a.boff[il + a.m_base], r, Tk, a.nphif, a.nb, a.nd,
-                                                         a.ndp, a.rph, a.rdb, a.rdd, a.offd);
-                    split_double(v, vB, vE);
-                    vE += lwv;
-                }
-                vS = 1.f;
-            }
-            // boundary point of the templates whose lowest point is this node
-            const int bs = use ? (int)bslot[tr] : -1;
-            float cB = -1e30f, cE = 0.f, cS = 0.f;
-            if (__any_sync(0xffffffffu, bs >= 0)) {
-                if (bs >= 0) {
-                    ++n_bnd;
-                    const float sfr = fb + bcf[bs];
-                    const int cy = sfr >= 1.f;
-                    const float fbf = cy ? sfr - 1.f : sfr;
-                    const int b0 = ibh + bci[bs] + cy;
-                    const int rb = b0 - R0, rd = d0 - C0;
-                    const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) &&
-                                      (unsigned)rd <= (unsigned)(EXM_WD - 2) && b0 <= a.nb - 2 &&
-                                      !(b0 == a.nb - 2 && fbf > 0.999999f);
-                    if (fast) {
-                        interp_window(s0, s1, rb * EXM_WD + rd, fbf, fd, w, cB, cE);
-                    } else {
-                        const int t = tsr[j];
-                        int i1 = t + tau0;
-                        if (i1 >= nt) i1 -= nt;
-                        const int gi = il + a.m_base;
-                        const double v = exm_tap_fp64<float>(a.L[(long long)il * nt + t], a.H[(long long)il * nt + i1],
-                                                             a.cb[gi] + a.boff[gi], r, Tk, a.nphif, a.nb, a.nd, a.ndp,
-                                                             a.rph, a.rdb, a.rdd, a.offd);
-                        split_double(v, cB, cE);
-                    }
-                    cE += lwv;
-                    cS = 1.f;
-                }
-                const bool hb = seg_reduce(bs >= 0 ? bs : -2 - lane, cB, cE, cS);
-                if (hb && bs >= 0) {
-                    float B = bB[bs], E = bE[bs], S = bS[bs];
-                    lse_merge(B, E, S, cB, cE, cS);
-                    bB[bs] = B;
-                    bE[bs] = E;
-                    bS[bs] = S;
-                }
-            }
-            const bool head = seg_reduce(tr, vB, vE, vS);
-            if (head && use) {
-                float B = aB[tr], E = aE[tr], S = aS[tr];
-                lse_merge(B, E, S, vB, vE, vS);
-                aB[tr] = B;
-                aE[tr] = E;
-                aS[tr] = S;
-            }
+        rc.s0 = win + (p % 3) * SLOT_FLOATS;
+        rc.s1 = win + ((p + 1) % 3) * SLOT_FLOATS;
+        const int *offp = offr + p * (a.nmc + 1) + base_i;
+        rc.aB = aB;
+        rc.aE = aE;
+        rc.aS = aS;
+        process_run<false>(a, rc, offp[wa], offp[wb], n_slow);
+        if (ib0 < ib1) {
+            rc.aB = bB;
+            rc.aE = bE;
+            rc.aS = bS;
+            const int bb = offp[ib0], be = offp[ib1];
+            n_bnd += (lane == 0) ? (unsigned)(be - bb) : 0u;
+            process_run<true>(a, rc, bb, be, n_slow);
         }
-        if (a.stats) {
-            const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);
-            if (lane == 0 && (sl_ | bd_)) {
-                atomicAdd(&a.stats[0], (unsigned long long)sl_);
-                atomicAdd(&a.stats[1], (unsigned long long)bd_);
-            }
+    }
+    if (a.stats) {
+        const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);
+        if (lane == 0 && (sl_ | bd_)) {
+            atomicAdd(&a.stats[0], (unsigned long long)sl_);
+            atomicAdd(&a.stats[1], (unsigned long long)bd_);
         }
     }
     __syncthreads();
@@ -345,10 +395,9 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         const float S = aS[j];
         const double v = (ok && S > 0.f) ? (double)aB[j] + (double)aE[j] + log((double)S) : -INFINITY;
         a.part[((long long)k * a.ntau + r) * a.nm_total + lo + j] = v;
-        const int bs = bslot[j];
-        if (bs >= 0) {
-            const float S2 = bS[bs];
-            const double v2 = (ok && S2 > 0.f) ? (double)bB[bs] + (double)bE[bs] + log((double)S2) : -INFINITY;
+        if (j >= blo && j < bhi && a.bnode[lo + j] == k) {
+            const float S2 = bS[j];
+            const double v2 = (ok && S2 > 0.f) ? (double)bB[j] + (double)bE[j] + log((double)S2) : -INFINITY;
             a.part[((long long)a.nn * a.ntau + r) * a.nm_total + lo + j] = v2;
         }
     }
@@ -356,9 +405,9 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 
 #define GATHER_NW 16
 
-static size_t planes_smem()
+static size_t planes_smem(int tch)
 {
-    return (size_t)3 * SLOT_BYTES + 64 + (size_t)EXM_TCH * (8 * 4 + 2);
+    return (size_t)3 * SLOT_BYTES + 64 + (size_t)tch * 8 * 4;
 }
 
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc)
@@ -406,16 +455,24 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
         a.cki[k] = (int)f;
         a.ckf[k] = (float)(ctx->ck[k] - f);
     }
-    // blocks of up to EXM_TCH templates: as many as the widest node range needs
+    // templates per block: about one wave of blocks per lag, so that the descriptors of the lag
+    // in flight stay in L2; at most EXM_TCH (shared-memory accumulators)
+    long long pairs = 0;
     int maxn = 0;
     for (int k = 0; k < ctx->nn; ++k) {
         const int lo = std::max(ctx->mlo[k], ci.m_base), hi = std::min(ctx->mhi[k], ci.m_base + ci.nmc);
+        pairs += std::max(0, hi - lo);
         maxn = std::max(maxn, hi - lo);
     }
     if (maxn <= 0) return;
-    const size_t smem = planes_smem();
+    int tch = (int)((pairs + ctx->sm_count - 1) / ctx->sm_count);
+    tch = std::max(tch, 256);
+    tch = std::min(((tch + 15) / 16) * 16, EXM_TCH);
+    a.tch = tch;
+    a.nch = (maxn + tch - 1) / tch;
+    const size_t smem = planes_smem(tch);
     EXM_CUDA(cudaFuncSetAttribute(k_gather_planes<GATHER_NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(rc * ctx->nn, (maxn + EXM_TCH - 1) / EXM_TCH);
+    dim3 grid(rc * ctx->nn * a.nch);
     k_gather_planes<GATHER_NW><<<grid, GATHER_NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
     EXM_CUDA(cudaGetLastError());
     // algorithmic work of this launch: one node-tap per (template slot, lag, walked time)
