@@ -88,14 +88,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsign
 
 __device__ __forceinline__ void lse_merge(float &B, float &E, float &S, float B2, float E2, float S2)
 {
+    // (B, E, S) += (B2, E2, S2): the larger of the two values becomes the reference, without a branch
     const float d = (B2 - B) + (E2 - E);
-    if (d > 0.f) {
-        S = fmaf(S, __expf(-d), S2);
-        B = B2;
-        E = E2;
-    } else {
-        S = fmaf(S2, __expf(d), S);
-    }
+    const bool up = d > 0.f;
+    const float e = __expf(-fabsf(d));
+    const float s_up = fmaf(S, e, S2), s_dn = fmaf(S2, e, S);
+    B = up ? B2 : B;
+    E = up ? E2 : E;
+    S = up ? s_up : s_dn;
 }
 
 // segmented reduction over lanes with equal id (ids non-decreasing along the lanes of a run);
@@ -196,61 +196,117 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
     c.aS[tr] = s;
 }
 
+#define TPL 4   // consecutive taps per lane (groups of GRP); a warp chunk is 32 * TPL taps
+#define GRP 4
+
+// the lane-local running segmented merge of one value (taps arrive sorted by template)
+__device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
+                                           float &cS, int &fT, float &fB, float &fE, float &fS)
+{
+    const float vS = t >= 0 ? 1.f : 0.f;
+    const bool same = (t == cT);
+    if (!same && cT >= 0) {   // cT closes here: the lane's first closed partial, or one inside the lane
+        if (fT < 0) {
+            fT = cT;
+            fB = cB;
+            fE = cE;
+            fS = cS;
+        } else {
+            acc_merge(c, cT, cB, cE, cS);
+        }
+    }
+    if (same) {
+        lse_merge(cB, cE, cS, vB, vE, vS);
+    } else {
+        cT = t;
+        cB = vB;
+        cE = vE;
+        cS = vS;
+    }
+}
+
+// GRP taps: decode, window interpolation for all of them (no branch between the shared loads),
+// the exact float64 value for the rare taps outside the window, then the merges
+template <bool BND>
+__device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, const uint4 *q, int j, int end, int &cT,
+                                          float &cB, float &cE, float &cS, int &fT, float &fB, float &fE, float &fS,
+                                          unsigned &n_slow)
+{
+    int t[GRP], o[GRP];
+    bool fast[GRP];
+    float fbf[GRP], fd[GRP], w[GRP], lwv[GRP], vB[GRP], vE[GRP];
+#pragma unroll
+    for (int u = 0; u < GRP; ++u) {
+        int tt = (j + u < end) ? (int)(q[u].w >> 19) + c.m_base - c.lo : -1;
+        if (tt >= c.n) {   // outside the block's templates: report and skip
+            atomicOr(a.err, EXM_DEVERR_BOUNDS);
+            tt = -1;
+        }
+        if (BND && tt >= 0 && c.bnode[tt + c.lo] != c.k) tt = -1;
+        t[u] = tt;
+        const int ts = tt >= 0 ? tt : 0;
+        const float fb = __uint_as_float(q[u].x);
+        fd[u] = __uint_as_float(q[u].y);
+        w[u] = __uint_as_float(q[u].z & 0x7FFFFFFFu);
+        lwv[u] = (q[u].z >> 31) ? c.lw : 0.f;
+        const int d0 = (int)((q[u].w >> 11) & 0xFFu);
+        const int ibh = ((int)(q[u].w << 21)) >> 21;
+        const float sfr = fb + (BND ? c.bcf[ts] : c.ckf);
+        const int cy = sfr >= 1.f;
+        fbf[u] = cy ? sfr - 1.f : sfr;
+        const int b0 = ibh + (BND ? c.bci[ts] : c.cki) + cy;
+        const int rb = b0 - c.R0, rd = d0 - c.C0;
+        fast[u] = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
+                  b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf[u] > 0.999999f);
+        o[u] = min(max(rb, 0), EXM_WB - 2) * EXM_WD + min(max(rd, 0), EXM_WD - 2);
+    }
+#pragma unroll
+    for (int u = 0; u < GRP; ++u) interp_window(c.s0, c.s1, o[u], fbf[u], fd[u], w[u], vB[u], vE[u]);
+#pragma unroll
+    for (int u = 0; u < GRP; ++u) {
+        if (t[u] >= 0 && !fast[u]) {
+            ++n_slow;
+            const int il = (int)(q[u].w >> 19);
+            const int tm = c.tsr[j + u];
+            int i1 = tm + c.tau0;
+            if (i1 >= c.nt) i1 -= c.nt;
+            const int gi = il + c.m_base;
+            const double offb = (BND ? a.cb[gi] : c.offb_node) + a.boff[gi];
+            const double v = exm_tap_fp64<float>(a.L[(long long)il * c.nt + tm], a.H[(long long)il * c.nt + i1], offb,
+                                                 c.r, a.T + (long long)c.k * a.tstride, a.nphif, a.nb, a.nd, a.ndp,
+                                                 a.rph, a.rdb, a.rdd, a.offd);
+            split_double(v, vB[u], vE[u]);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < GRP; ++u) lane_merge(c, t[u], vB[u], vE[u] + lwv[u], cT, cB, cE, cS, fT, fB, fE, fS);
+}
+
 template <bool BND>
 __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
 {
     const int lane = threadIdx.x & 31;
-    uint4 qn[4];
-    int jn = beg + 4 * lane;
+    uint4 qa[GRP];
+    int jb = beg + TPL * lane;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) qn[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
-    for (int j0 = beg; j0 < end; j0 += 128) {
-        uint4 q[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) q[u] = qn[u];
-        const int jb = j0 + 4 * lane;
-        jn = jb + 128;
-        if (j0 + 128 < end) {   // prefetch the next chunk
-#pragma unroll
-            for (int u = 0; u < 4; ++u) qn[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
-        }
-        int tr[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            int t = (jb + u < end) ? (int)(q[u].w >> 19) + c.m_base - c.lo : -1;
-            if (t >= c.n) {   // outside the block's templates: report and skip
-                atomicOr(a.err, EXM_DEVERR_BOUNDS);
-                t = -1;
-            }
-            if (BND && t >= 0 && c.bnode[t + c.lo] != c.k) t = -1;
-            tr[u] = t;
-        }
-        // lane-local merge of the 4 taps; cT is the lane's last template, fT its first closed one
+    for (int u = 0; u < GRP; ++u) qa[u] = (jb + u < end) ? __ldg(c.descr + jb + u) : make_uint4(0u, 0u, 0u, 0u);
+    for (int j0 = beg; j0 < end; j0 += 32 * TPL) {
+        jb = j0 + TPL * lane;
         int cT = -1, fT = -1;
         float cB = -1e30f, cE = 0.f, cS = 0.f, fB = -1e30f, fE = 0.f, fS = 0.f;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (tr[u] < 0) continue;
-            float vB, vE;
-            tap_value<BND>(a, c, q[u], jb + u, tr[u], vB, vE, n_slow);
-            if (tr[u] == cT) {
-                lse_merge(cB, cE, cS, vB, vE, 1.f);
-            } else {
-                if (cT >= 0) {
-                    if (fT < 0) {
-                        fT = cT;
-                        fB = cB;
-                        fE = cE;
-                        fS = cS;
-                    } else {
-                        acc_merge(c, cT, cB, cE, cS);   // lies inside this lane's taps
-                    }
-                }
-                cT = tr[u];
-                cB = vB;
-                cE = vE;
-                cS = 1.f;
+        for (int g = 0; g < TPL / GRP; ++g) {
+            uint4 cur[GRP];
+#pragma unroll
+            for (int u = 0; u < GRP; ++u) cur[u] = qa[u];
+            // the next group of descriptors (this lane's next group, or the next chunk's first)
+            const int jn = (g + 1 < TPL / GRP) ? jb + (g + 1) * GRP : jb + 32 * TPL;
+            if (g + 1 < TPL / GRP || j0 + 32 * TPL < end) {
+#pragma unroll
+                for (int u = 0; u < GRP; ++u)
+                    qa[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
             }
+            tap_group<BND>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
         }
         // the first closed template of lane l + 1 continues lane l's last one, or is lane l + 1's alone
         const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
