@@ -21,7 +21,7 @@ PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_ctx_timing", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
-           "exm_gather", "exm_node_values")
+           "exm_gather", "exm_node_values", "exm_gather_noalloc")
 
 _lib = None
 
@@ -60,6 +60,7 @@ def load():
         "exm_set_times": ([P, I, P, P], I),
         "exm_gather": ([P, I, I, P, P, P, P], I),
         "exm_node_values": ([P, P], I),
+        "exm_gather_noalloc": ([P, I, I, P, P, P, P, I, P, P, I, I, P, P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -222,6 +223,14 @@ class Context:
         out = np.empty((ns, nsel), np.float64)
         self._check(self.lib.exm_gather(self.h, nsel, ns, _p(ids), _p(lna), _p(tab), _p(out)))
         return out
+
+    def gather_noalloc(self, nm, n_time, lqH, phH, lqL, phL, nwalk, sel, lw, nsel, ns, mass_ids, lna, tab_ids, out):
+        """exm_gather_noalloc: every argument after n_time is a device address (int) the caller owns;
+        the call allocates no device memory"""
+        P = ctypes.c_void_p
+        self._check(self.lib.exm_gather_noalloc(self.h, int(nm), int(n_time), P(lqH), P(phH), P(lqL), P(phL),
+                                                int(nwalk), P(sel) if sel else None, P(lw) if lw else None,
+                                                int(nsel), int(ns), P(mass_ids), P(lna), P(tab_ids), P(out)))
 
     def node_values(self, n_nodes):
         out = np.empty((n_nodes + 1, self.nm), np.float64)

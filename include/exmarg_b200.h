@@ -160,6 +160,25 @@ EXM_API int exm_set_times(exm_ctx *ctx, int nwalk, const int32_t *sel, const flo
 EXM_API int exm_gather(exm_ctx *ctx, int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,
                double *out);
 
+/* The float64 gather of exm_gather for callers that cannot allocate device memory
+ * during the call (a framework whose memory pool owns the device, a spent budget, a
+ * context where an allocation would synchronise).  No counterpart in the reference.
+ * Every argument is a device pointer the caller owns: lqH, phH, lqL, phL (nm, n_time)
+ * float32 trajectories; sel, lw (nm, nwalk) visited times and their log weights
+ * (nwalk = 0: every time); mass_ids (nsel) int64, lna (nsel, ns) float64, tab_ids
+ * (nsel, ns) int64 node indices into the context's resident store; out (ns, nsel)
+ * float64.  The call allocates nothing: its partial sums live in a fixed device array
+ * of the library (16 MiB, held by every device that loads the library), so
+ * ns * n_lag * nsel must not exceed 2^20 (larger requests fail with EXM_ERR_ARG).  The
+ * first call on a device looks the array's device address up (cudaGetSymbolAddress);
+ * make it before any stream capture.  Calls share the array: two calls that overlap on
+ * the GPU race.  It runs on the context's stream and returns after the result is
+ * written. */
+EXM_API int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float *lqH, const float *phH,
+                               const float *lqL, const float *phL, int nwalk, const int32_t *sel, const float *lw,
+                               int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,
+                               double *out);
+
 /* Node values of the current segment (exmarg/search/pe.py:168-200,
  * _node_values): lamN_out (n_nodes + 1, nm) float64, -inf where a template does
  * not reach a node; row n_nodes the boundary point.  Uses the plane-staged gather. */
