@@ -71,7 +71,7 @@ def make_inputs(n_seg, rank, n_templates=N_TEMPLATES, n_nodes=53, n_lags=87):
 class ClockSampler:
     """nvidia-smi samples of one GPU during the timed region"""
 
-    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+    FIELDS = "timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
@@ -79,6 +79,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.window = None
 
     def start(self):
         try:
@@ -92,7 +93,11 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0, t1):
+        """the timed region, in time.time() seconds: only samples inside it are kept"""
+        self.window = (t0, t1)
 
     def stop(self):
         if self.proc is None:
@@ -104,17 +109,19 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if self.window and not (self.window[0] <= ts <= self.window[1] + 0.25):
+                continue
             parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-                power.append(float(parts[3]))
+                sm.append(float(parts[2]))
+                smax.append(float(parts[3]))
+                power.append(float(parts[4]))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            for n, v in zip(names, parts[6:10]):
                 if v.lower() == "active":
                     reasons.add(n)
         load = [s for s, p in zip(sm, power) if p > 200.0] or sm
@@ -218,15 +225,24 @@ def run_b200(args):
     store.generator = (M, P, Q, S, TABLE_SEED)
     eb.prepare(bank, store, "volume", 0.1267)
 
+    # the clock sampler starts before the warm-up: its start-up (NVML initialisation) holds the
+    # driver for a moment and must not fall inside the timed region
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(2.0)
     for i in range(args.warmup):
         eb.pe_intrinsic(seg, bank, store, rows=[i])
+    tune = None
+    if not args.no_tune:
+        best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
+        tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:5]],
+                "shapes": ["16w x4", "16w x2", "24w x2", "32w x2", "32w x1"]}
     ctx.timing(True)
     if pg:
         pg.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     lat = []
     res = []
+    tw0 = time.time()
     t0 = time.perf_counter()
     for i in range(args.warmup, n_seg):
         a = time.perf_counter()
@@ -234,6 +250,7 @@ def run_b200(args):
         lat.append(time.perf_counter() - a)
         res.append(r)
     wall = time.perf_counter() - t0
+    clocks.mark(tw0, time.time())
     clk = clocks.stop()
     tm = ctx.timing(False)
     dev_s = tm["total_ms"] / 1000.0
@@ -268,7 +285,7 @@ def run_b200(args):
                          "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": g_ms,
                          "node_taps_per_launch": tm["node_taps"] / max(launches, 1),
                          "dram_gbs": (traffic / (g_ms / 1000.0) / 1e9) if traffic else None},
-            "gather_gbs_logical": achieved, "clocks": clk}
+            "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -302,6 +319,7 @@ def main():
     ap.add_argument("--cpu-templates", type=int, default=128)
     ap.add_argument("--ref-templates", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-tune", action="store_true", help="skip the gather launch-shape autotuner")
     ap.add_argument("--templates", type=int, default=N_TEMPLATES, help="bank size (reduced profiling cases)")
     ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
     ap.add_argument("--lags", type=int, default=87, help="table lags (reduced profiling cases; odd)")

@@ -13,9 +13,9 @@ ctypes; there is no CPU fallback on the 'b200' path.
 from .segments import D0, read_segments
 from .bank import MassBank, mass_bank, from_bank, array_module
 from .store import RedshiftStore, load_redshift_store, upload_store
-from .pe import pe_intrinsic, distance_weights, prepare
+from .pe import pe_intrinsic, distance_weights, prepare, autotune
 from ._lib import Context, context
 
 __all__ = ["D0", "read_segments", "MassBank", "mass_bank", "from_bank", "array_module", "RedshiftStore",
-           "load_redshift_store", "upload_store", "pe_intrinsic", "distance_weights", "prepare", "Context",
+           "load_redshift_store", "upload_store", "pe_intrinsic", "distance_weights", "prepare", "autotune", "Context",
            "context"]

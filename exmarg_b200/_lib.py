@@ -21,7 +21,7 @@ PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_ctx_timing", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
-           "exm_gather", "exm_node_values", "exm_gather_noalloc")
+           "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg")
 
 _lib = None
 
@@ -61,6 +61,8 @@ def load():
         "exm_gather": ([P, I, I, P, P, P, P], I),
         "exm_node_values": ([P, P], I),
         "exm_gather_noalloc": ([P, I, I, P, P, P, P, I, P, P, I, I, P, P, P, P], I),
+        "exm_autotune": ([P, I, I, I, P, P], I),
+        "exm_set_gather_cfg": ([P, I], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -232,10 +234,36 @@ class Context:
                                                 int(nwalk), P(sel) if sel else None, P(lw) if lw else None,
                                                 int(nsel), int(ns), P(mass_ids), P(lna), P(tab_ids), P(out)))
 
+    def autotune(self, n_loud=1024, n_random=1024, reps=2):
+        """time every launch shape of the plane gather on the last segment; keep the fastest.
+        returns (best index, ms per launch of each shape)"""
+        best = ctypes.c_int()
+        ms = np.zeros(16, np.float64)
+        self._check(self.lib.exm_autotune(self.h, int(n_loud), int(n_random), int(reps), ctypes.byref(best), _p(ms)))
+        return best.value, ms
+
+    def set_gather_cfg(self, cfg):
+        self._check(self.lib.exm_set_gather_cfg(self.h, int(cfg)))
+
     def node_values(self, n_nodes):
         out = np.empty((n_nodes + 1, self.nm), np.float64)
         self._check(self.lib.exm_node_values(self.h, _p(out)))
         return out
+
+
+_tokens = iter(range(1, 1 << 62))
+
+
+def token_of(obj):
+    """a process-unique token for a bank or store object (id() values are reused after collection)"""
+    t = getattr(obj, "_b200_token", None)
+    if t is None:
+        t = next(_tokens)
+        try:
+            object.__setattr__(obj, "_b200_token", t)
+        except (AttributeError, TypeError):
+            obj.__dict__["_b200_token"] = t
+    return t
 
 
 _contexts = {}

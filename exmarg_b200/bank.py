@@ -82,9 +82,10 @@ class MassBank:
     def upload(self):
         """make this bank the context's current bank (W copied to HBM)"""
         ctx = self.ctx
-        if ctx.bank_token != id(self):
+        token = _lib.token_of(self)
+        if ctx.bank_token != token:
             ctx.bank_set(self.W, self.lo, self.n_time, self.u, self.M, self.q, self.chi)
-            ctx.bank_token = id(self)
+            ctx.bank_token = token
             ctx.prep_token = None
         return ctx
 

@@ -673,6 +673,62 @@ extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, cons
         for (int i = 0; i < ctx->nm; ++i) ln_lambda[(size_t)e * ctx->nm + ctx->order[i]] = lnl[i];
     }
     ctx->traj_ok = ctx->times_ok = false;
+    ctx->last_shape_ok = n_seg > 0;
+    API_END(ctx)
+}
+
+// ------------------------------------------------------------------ autotuner
+
+extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, double *ms_per_cfg)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->prep_ok, EXM_ERR_STATE, "exm_pe_prepare first");
+    REQUIRE(ctx->last_shape_ok, EXM_ERR_STATE, "run exm_pe_intrinsic once first (the autotuner replays its last segment)");
+    const RunShape rs = run_shape(ctx, n_loud, n_random);
+    REQUIRE(rs.nmc_max >= ctx->nm && rs.rc >= ctx->ntau, EXM_ERR_ARG,
+            "the autotuner needs the whole bank and every lag in one gather (bank <= 8192 templates)");
+    exm_slot &sl = ctx->slot;
+    ChunkInfo ci{0, ctx->nm, rs.nwalk, rs.use_sel, rs.lw};
+    const int n = exm_gather_num_cfgs();
+    cudaEvent_t e0, e1;
+    EXM_CUDA(cudaEventCreate(&e0));
+    EXM_CUDA(cudaEventCreate(&e1));
+    const int keep = ctx->gather_cfg;
+    const bool tim = ctx->tim_on;
+    ctx->tim_on = false;
+    double best = 1e300;
+    int arg = keep;
+    for (int c = 0; c < n; ++c) {
+        ctx->gather_cfg = c;
+        exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);   // warm-up (and function attributes)
+        EXM_CUDA(cudaEventRecord(e0, ctx->stream));
+        for (int r = 0; r < std::max(1, reps); ++r) exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);
+        EXM_CUDA(cudaEventRecord(e1, ctx->stream));
+        EXM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        EXM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const double per = ms / std::max(1, reps);
+        if (ms_per_cfg) ms_per_cfg[c] = per;
+        if (per < best) {
+            best = per;
+            arg = c;
+        }
+    }
+    ctx->tim_on = tim;
+    ctx->gather_cfg = arg;
+    if (best_cfg) *best_cfg = arg;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_dev_err(ctx, sl);
+    API_END(ctx)
+}
+
+extern "C" int exm_set_gather_cfg(exm_ctx *ctx, int cfg)
+{
+    API_BEGIN(ctx)
+    REQUIRE(cfg >= 0 && cfg < exm_gather_num_cfgs(), EXM_ERR_ARG, "no such gather launch shape");
+    ctx->gather_cfg = cfg;
     API_END(ctx)
 }
 

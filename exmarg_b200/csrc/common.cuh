@@ -118,6 +118,9 @@ struct exm_ctx {
     dbuf d_ckd;                       // double [EXM_MAX_NODES]: ck
     dbuf d_stats;                     // uint64 [4]: gather counters (slow-path taps, boundary taps)
 
+    // launch shape of the plane gather (index into its table; chosen by exm_autotune)
+    int gather_cfg = 0;
+
     // cuFFT
     cufftHandle plan = 0;
     int plan_batch = 0, plan_n = 0;
@@ -134,7 +137,7 @@ struct exm_ctx {
 
     // current segment state for the stage entry points
     exm_slot slot;
-    bool traj_ok = false, times_ok = false;
+    bool traj_ok = false, times_ok = false, last_shape_ok = false;
     int cur_nwalk = 0;
     float cur_lw = 0.f;
     std::vector<exm_slot> slots;

@@ -196,38 +196,34 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
     c.aS[tr] = s;
 }
 
-#define TPL 4   // consecutive taps per lane (groups of GRP); a warp chunk is 32 * TPL taps
-#define GRP 4
+#define TPL 4   // consecutive taps per lane (in groups of GRP); a warp chunk is 32 * TPL taps
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
                                            float &cS, int &fT, float &fB, float &fE, float &fS)
 {
-    const float vS = t >= 0 ? 1.f : 0.f;
-    const bool same = (t == cT);
-    if (!same && cT >= 0) {   // cT closes here: the lane's first closed partial, or one inside the lane
-        if (fT < 0) {
-            fT = cT;
-            fB = cB;
-            fE = cE;
-            fS = cS;
-        } else {
-            acc_merge(c, cT, cB, cE, cS);
+    if (t != cT) {
+        if (cT >= 0) {   // cT closes here: the lane's first closed partial, or one inside the lane
+            if (fT < 0) {
+                fT = cT;
+                fB = cB;
+                fE = cE;
+                fS = cS;
+            } else {
+                acc_merge(c, cT, cB, cE, cS);
+            }
         }
+        cT = t;          // an empty partial: the merge below makes it (vB, vE, vS)
+        cB = -1e30f;
+        cE = 0.f;
+        cS = 0.f;
     }
-    if (same) {
-        lse_merge(cB, cE, cS, vB, vE, vS);
-    } else {
-        cT = t;
-        cB = vB;
-        cE = vE;
-        cS = vS;
-    }
+    lse_merge(cB, cE, cS, vB, vE, t >= 0 ? 1.f : 0.f);
 }
 
 // GRP taps: decode, window interpolation for all of them (no branch between the shared loads),
 // the exact float64 value for the rare taps outside the window, then the merges
-template <bool BND>
+template <bool BND, int GRP>
 __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, const uint4 *q, int j, int end, int &cT,
                                           float &cB, float &cE, float &cS, int &fT, float &fB, float &fE, float &fS,
                                           unsigned &n_slow)
@@ -282,7 +278,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
     for (int u = 0; u < GRP; ++u) lane_merge(c, t[u], vB[u], vE[u] + lwv[u], cT, cB, cE, cS, fT, fB, fE, fS);
 }
 
-template <bool BND>
+template <bool BND, int GRP>
 __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
 {
     const int lane = threadIdx.x & 31;
@@ -306,7 +302,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
                 for (int u = 0; u < GRP; ++u)
                     qa[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
             }
-            tap_group<BND>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
+            tap_group<BND, GRP>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
         }
         // the first closed template of lane l + 1 continues lane l's last one, or is lane l + 1's alone
         const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
@@ -322,7 +318,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
     }
 }
 
-template <int NW>
+template <int NW, int GRP>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -424,14 +420,14 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         rc.aB = aB;
         rc.aE = aE;
         rc.aS = aS;
-        process_run<false>(a, rc, offp[wa], offp[wb], n_slow);
+        process_run<false, GRP>(a, rc, offp[wa], offp[wb], n_slow);
         if (ib0 < ib1) {
             rc.aB = bB;
             rc.aE = bE;
             rc.aS = bS;
             const int bb = offp[ib0], be = offp[ib1];
             n_bnd += (lane == 0) ? (unsigned)(be - bb) : 0u;
-            process_run<true>(a, rc, bb, be, n_slow);
+            process_run<true, GRP>(a, rc, bb, be, n_slow);
         }
     }
     if (a.stats) {
@@ -459,7 +455,32 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     }
 }
 
-#define GATHER_NW 16
+// launch shapes the autotuner chooses from: (warps per block, taps per register group)
+struct GatherCfg {
+    int nw, grp;
+};
+static const GatherCfg kGatherCfgs[] = {{16, 4}, {16, 2}, {24, 2}, {32, 2}, {32, 1}};
+static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
+
+template <int NW, int GRP>
+static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
+{
+    EXM_CUDA(cudaFuncSetAttribute(k_gather_planes<NW, GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gather_planes<NW, GRP><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+}
+
+static void launch_cfg(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
+{
+    switch (cfg) {
+    case 0: launch_planes<16, 4>(ctx, a, grid, smem); break;
+    case 1: launch_planes<16, 2>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 2>(ctx, a, grid, smem); break;
+    case 3: launch_planes<32, 2>(ctx, a, grid, smem); break;
+    default: launch_planes<32, 1>(ctx, a, grid, smem); break;
+    }
+}
+
+int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 
 static size_t planes_smem(int tch)
 {
@@ -527,9 +548,9 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.tch = tch;
     a.nch = (maxn + tch - 1) / tch;
     const size_t smem = planes_smem(tch);
-    EXM_CUDA(cudaFuncSetAttribute(k_gather_planes<GATHER_NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid(rc * ctx->nn * a.nch);
-    k_gather_planes<GATHER_NW><<<grid, GATHER_NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+    const int cfg = (ctx->gather_cfg >= 0 && ctx->gather_cfg < kNumGatherCfgs) ? ctx->gather_cfg : 0;
+    launch_cfg(ctx, cfg, a, grid, smem);
     EXM_CUDA(cudaGetLastError());
     // algorithmic work of this launch: one node-tap per (template slot, lag, walked time)
     double slots = 0;

@@ -7,7 +7,7 @@
 
 // staging window of one (node, lag, phase plane): rows of beta x columns of Delta
 #define EXM_WB 80
-#define EXM_WD 160
+#define EXM_WD 164   // row pitch = 4 banks mod 32: neighbouring rows start on different banks
 #define EXM_TCH 2048        // templates per gather block
 #define EXM_MAX_CHUNK 8192  // templates per pass (13-bit template field of a descriptor)
 #define EXM_MAX_NODES 64
@@ -118,6 +118,7 @@ struct ChunkInfo {
 };
 void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc, bool first_chunk_of_lags);
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc);
+int exm_gather_num_cfgs();
 void exm_run_node_lse(exm_ctx *ctx, exm_slot &sl, int m_base, int nmc);
 void exm_run_lnb(exm_ctx *ctx, exm_slot &sl);
 void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const int *d_rows, const int *d_tab,

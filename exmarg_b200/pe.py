@@ -18,13 +18,19 @@ from .segments import read_segments
 from .store import upload_store
 
 
+def _density_key(prior):
+    """a content key for a tabulated density (lny, p_lny)"""
+    a, b = (np.ascontiguousarray(x, np.float64) for x in prior)
+    return ("tabulated", a.size, hash(a.tobytes()), hash(b.tobytes()))
+
+
 def prepare(bank, store, prior="volume", ymin=0.1267):
     """make (store, bank, prior, ymin) current on the bank's context: tables resident, geometry and
     distance weights computed on the device (once; later calls with the same inputs reuse them)"""
     ctx = bank.ctx
     upload_store(store, ctx)
     bank.upload()
-    key = (ctx.store_token, ctx.bank_token, prior if isinstance(prior, str) else id(prior), float(ymin))
+    key = (ctx.store_token, ctx.bank_token, prior if isinstance(prior, str) else _density_key(prior), float(ymin))
     if ctx.prep_token != key:
         density = distance_density(prior)
         if density is None:
@@ -55,6 +61,14 @@ def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, 
     seeds = seed + np.asarray(seg["rows"], np.int64)
     lnl, lnb = ctx.pe_intrinsic(seg["d_H"], seg["d_L"], seg["sig2_H"], seg["sig2_L"], seeds, n_loud, n_random)
     return dict(M=bank.M, q=bank.q, chi=bank.chi, u=bank.u, ln_lambda=lnl, ln_b=lnb, rows=seg["rows"])
+
+
+def autotune(bank, store, segments, prior="volume", ymin=0.1267, n_loud=1024, n_random=1024, reps=2):
+    """choose the plane gather's launch shape for this bank and store: analyse the first segment
+    once, then time every shape on it (CUDA events); later calls on the context use the fastest.
+    returns (chosen shape index, ms per launch of each shape)"""
+    pe_intrinsic(segments, bank, store, rows=[0], prior=prior, ymin=ymin, n_loud=n_loud, n_random=n_random)
+    return bank.ctx.autotune(n_loud, n_random, reps)
 
 
 def distance_weights(y, prior, ymin):

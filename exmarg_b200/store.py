@@ -99,7 +99,7 @@ def store_grid(store):
 
 def upload_store(store, ctx):
     """copy the store's tables into the context's HBM once (skipped if this store is already resident)"""
-    token = id(store)
+    token = _lib.token_of(store)
     if ctx.store_token == token:
         return
     gen = getattr(store, "generator", None)

@@ -130,6 +130,17 @@ EXM_API int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const d
                      const double *sig2_L, const int64_t *seeds, int n_loud, int n_random, double *ln_lambda,
                      double *ln_b);
 
+/* Autotuner of the plane gather's launch shape (warps per block x taps per register
+ * group): replays the gather of the last segment analysed by exm_pe_intrinsic on this
+ * context (same n_loud, n_random) once per shape, times each with CUDA events (reps
+ * launches), keeps the fastest for later calls and writes its index to best_cfg and the
+ * ms per launch of every shape to ms_per_cfg (if not NULL; exm_gather_num_cfgs entries).
+ * No reference counterpart (the reference takes block as a kwarg, pe.py:289-290). */
+EXM_API int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, double *ms_per_cfg);
+
+/* Select a launch shape of the plane gather by index (as exm_autotune reports it). */
+EXM_API int exm_set_gather_cfg(exm_ctx *ctx, int cfg);
+
 /* ------------------------------------------------------------------ stages (tests, gather-level drop-in) */
 
 /* Matched filter of one segment (exmarg/search/bank.py:56-78, MassBank.trajectories):
