@@ -56,14 +56,28 @@ def dist_env():
     return rank, world, local
 
 
+def segment_seed(rank):
+    """first segment seed of a rank: every replica analyses its own segments"""
+    return SEG_SEED + 100000 * rank
+
+
+def combine_ranks(values, dist):
+    """the max over ranks of each value (device and wall seconds): the job ends with its slowest rank"""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def make_inputs(n_seg, rank, n_templates=N_TEMPLATES, n_nodes=53, n_lags=87):
     from exmarg_b200 import synth
     spec = synth.TableSpec(ntau=n_lags)
     s_nodes = synth.S_NODES_PROD
     if n_nodes < s_nodes.size:            # a reduced case keeps nodes every template reaches
         s_nodes = s_nodes[30:30 + n_nodes]
-    seg = synth.make_segments(n_seg, SEG_SEED + 100000 * rank, T=T_SEG, fmax=FMAX, snr=15.0, mc=25.0, q=0.8,
-                              chi=0.1)
+    seg = synth.make_segments(n_seg, segment_seed(rank), T=T_SEG, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
     rows = synth.make_bank(n_templates, BANK_SEED)
     return spec, s_nodes, seg, rows
 
@@ -255,10 +269,7 @@ def run_b200(args):
     tm = ctx.timing(False)
     dev_s = tm["total_ms"] / 1000.0
     if pg:
-        import torch
-        t = torch.tensor([dev_s, wall], dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_s, wall = float(t[0]), float(t[1])
+        dev_s, wall = combine_ranks([dev_s, wall], pg)
         pg.barrier()
     total = args.steps * world
     value = total / dev_s

@@ -47,4 +47,8 @@ def test_no_cpu_fallback_without_gpu():
             "else:\n    print('OPENED')\n")
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
                          cwd=os.path.dirname(os.path.dirname(HEADER)))
-    assert ("RAISED" in out.stdout) or ("OPENED" in out.stdout)
+    import torch
+    if torch.cuda.is_available():
+        assert "OPENED" in out.stdout
+    else:
+        assert "RAISED" in out.stdout        # no device: the call fails, nothing falls back to the CPU
