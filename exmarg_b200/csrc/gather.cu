@@ -151,6 +151,8 @@ struct RunCtx {
     int lo, m_base, n, R0, C0, cki, k, r, tau0, nt;
     float ckf, lw;
     double offb_node;           // (ln s_k - beta0)/dbeta, regular runs
+    int tF, tL;                 // the templates at the two ends of this warp's taps (may be shared with
+    float *eF, *eL;             // neighbouring warps): their partials go to this warp's edge slots
 };
 
 template <bool BND>
@@ -189,11 +191,25 @@ __device__ __forceinline__ void tap_value(const PlaneArgs &a, const RunCtx &c, u
 
 __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, float E, float S)
 {
-    float b = c.aB[tr], e = c.aE[tr], s = c.aS[tr];
+    float *pB, *pE, *pS;
+    if (tr == c.tF) {
+        pB = c.eF;
+        pE = c.eF + 1;
+        pS = c.eF + 2;
+    } else if (tr == c.tL) {
+        pB = c.eL;
+        pE = c.eL + 1;
+        pS = c.eL + 2;
+    } else {
+        pB = c.aB + tr;
+        pE = c.aE + tr;
+        pS = c.aS + tr;
+    }
+    float b = *pB, e = *pE, s = *pS;
     lse_merge(b, e, s, B, E, S);
-    c.aB[tr] = b;
-    c.aE[tr] = e;
-    c.aS[tr] = s;
+    *pB = b;
+    *pE = e;
+    *pS = s;
 }
 
 #define TPL 4   // consecutive taps per lane (in groups of GRP); a warp chunk is 32 * TPL taps
@@ -318,6 +334,87 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
     }
 }
 
+// the template of descriptor j (block-local), or -1
+__device__ __forceinline__ int desc_template(const RunCtx &c, int j)
+{
+    return (int)(__ldg(&c.descr[j].w) >> 19) + c.m_base - c.lo;
+}
+
+// fold the warps' edge partials into the accumulators: one warp, lane w holding warp w's first (F)
+// and last (L) partials; templates ascend along the warps, so this is the lane-level merge again
+__device__ __forceinline__ void fold_edges(float *edge, int nw, float *aB, float *aE, float *aS, int n)
+{
+    const int lane = threadIdx.x & 31;
+    float fB = -1e30f, fE = 0.f, fS = 0.f, cB = -1e30f, cE = 0.f, cS = 0.f;
+    int fT = -1, cT = -1;
+    if (lane < nw) {
+        const float *e = edge + 8 * lane;
+        fT = __float_as_int(e[3]);
+        fB = e[0];
+        fE = e[1];
+        fS = e[2];
+        cT = __float_as_int(e[7]);
+        cB = e[4];
+        cE = e[5];
+        cS = e[6];
+        if (!(fT >= 0 && fT < n && fS > 0.f)) fT = -1;
+        if (!(cT >= 0 && cT < n)) cT = -1;
+    }
+    const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
+    const float nB = __shfl_down_sync(0xffffffffu, fB, 1);
+    const float nE = __shfl_down_sync(0xffffffffu, fE, 1);
+    const float nS = __shfl_down_sync(0xffffffffu, fS, 1);
+    const int pT = __shfl_up_sync(0xffffffffu, cT, 1);
+    if (lane < 31 && nT >= 0 && nT == cT) lse_merge(cB, cE, cS, nB, nE, nS);
+    if (fT >= 0 && !(lane > 0 && pT == fT)) {
+        float b = aB[fT], x = aE[fT], q = aS[fT];
+        lse_merge(b, x, q, fB, fE, fS);
+        aB[fT] = b;
+        aE[fT] = x;
+        aS[fT] = q;
+    }
+    const bool head = seg_reduce(cT >= 0 ? cT : -2 - lane, cB, cE, cS);
+    if (head && cT >= 0 && cS > 0.f) {
+        float b = aB[cT], x = aE[cT], q = aS[cT];
+        lse_merge(b, x, q, cB, cE, cS);
+        aB[cT] = b;
+        aE[cT] = x;
+        aS[cT] = q;
+    }
+}
+
+// this warp's equal share [w0, w1) of the run [beg, end), with its edge templates and slots
+template <bool BND, int GRP, int NW>
+__device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, float *edge,
+                                           unsigned &n_slow)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w0 = beg + (int)((long long)(end - beg) * warp / NW);
+    const int w1 = beg + (int)((long long)(end - beg) * (warp + 1) / NW);
+    float *e = edge + 8 * warp;
+    int tF = -1, tL = -1;
+    if (w0 < w1) {
+        tF = desc_template(c, w0);
+        tL = desc_template(c, w1 - 1);
+    }
+    if (lane == 0) {
+        e[0] = -1e30f;
+        e[1] = 0.f;
+        e[2] = 0.f;
+        e[3] = __int_as_float(tF == tL ? -1 : tF);
+        e[4] = -1e30f;
+        e[5] = 0.f;
+        e[6] = 0.f;
+        e[7] = __int_as_float(tL);
+    }
+    __syncwarp();
+    c.tF = (tF == tL) ? -1 : tF;   // one template only: the L slot takes it all
+    c.tL = tL;
+    c.eF = e;
+    c.eL = e + 4;
+    if (w0 < w1) process_run<BND, GRP>(a, c, w0, w1, n_slow);
+}
+
 template <int NW, int GRP>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
 {
@@ -330,6 +427,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     float *bB = aS + tch, *bE = bB + tch, *bS = bE + tch;
     float *bcf = bS + tch;
     int *bci = (int *)(bcf + tch);
+    __shared__ float edge[2][8 * NW];   // per warp: F partial + id, L partial + id (regular, boundary)
 
     // block -> (lag, node, template chunk), lags outermost so the blocks of one lag run together
     const int c_idx = blockIdx.x % a.nch;
@@ -340,7 +438,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     const int hi = min(hi0, lo + tch);
     if (lo >= hi) return;
     const int n = hi - lo;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
 
     // accumulators; the boundary range [blo, bhi) of the templates whose lowest point is node k
     __shared__ int bl_sh[2];
@@ -378,13 +476,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     }
     int issued = 2;
 
-    const int wa = (int)((long long)n * warp / NW), wb = (int)((long long)n * (warp + 1) / NW);   // block-local
     const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
     const int nt = a.nt;
     RunCtx rc;
     rc.descr = a.desc + (long long)rl * a.per_lag;
     rc.tsr = a.tside + (long long)rl * a.per_lag;
-    rc.bci = bci - 0;
+    rc.bci = bci;
     rc.bcf = bcf;
     rc.bnode = a.bnode;
     rc.lo = lo;
@@ -400,13 +497,19 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     rc.nt = nt;
     rc.lw = a.lw;
     rc.offb_node = a.ckd[k];
-    const int ib0 = max(wa, blo), ib1 = min(wb, bhi);   // this warp's boundary templates
-    const int base_i = lo - a.m_base;                    // chunk-local index of template lo
+    const int base_i = lo - a.m_base;   // chunk-local index of template lo
 
     unsigned n_slow = 0, n_bnd = 0;
     bool ok = mbar_wait(&mbar[0], 0, a.err);
     for (int p = 0; p < EXM_NPAIR; ++p) {
-        if (p > 0) __syncthreads();   // every warp is done with plane p - 1: its slot can be refilled
+        if (p > 0) {
+            __syncthreads();   // every warp is done with plane p - 1: its slot can be refilled,
+            if (tid < 32) {    // and the edge partials of that pair go into the accumulators
+                fold_edges(edge[0], NW, aB, aE, aS, n);
+                if (blo < bhi) fold_edges(edge[1], NW, bB, bE, bS, n);
+            }
+            __syncthreads();
+        }
         if (tid == 0 && ok && p + 2 < a.nphif) {
             const int q = p + 2;
             tma_load_plane(&tmap, &mbar[q % 3], win + (q % 3) * SLOT_FLOATS, C0, R0, q, r, k, SLOT_BYTES);
@@ -420,15 +523,20 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         rc.aB = aB;
         rc.aE = aE;
         rc.aS = aS;
-        process_run<false, GRP>(a, rc, offp[wa], offp[wb], n_slow);
-        if (ib0 < ib1) {
+        warp_share<false, GRP, NW>(a, rc, offp[0], offp[n], edge[0], n_slow);
+        if (blo < bhi) {
             rc.aB = bB;
             rc.aE = bE;
             rc.aS = bS;
-            const int bb = offp[ib0], be = offp[ib1];
-            n_bnd += (lane == 0) ? (unsigned)(be - bb) : 0u;
-            process_run<true, GRP>(a, rc, bb, be, n_slow);
+            const int bb = offp[blo], be = offp[bhi];
+            n_bnd += (lane == 0 && (tid >> 5) == 0) ? (unsigned)(be - bb) : 0u;
+            warp_share<true, GRP, NW>(a, rc, bb, be, edge[1], n_slow);
         }
+    }
+    __syncthreads();
+    if (tid < 32 && ok) {
+        fold_edges(edge[0], NW, aB, aE, aS, n);
+        if (blo < bhi) fold_edges(edge[1], NW, bB, bE, bS, n);
     }
     if (a.stats) {
         const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);

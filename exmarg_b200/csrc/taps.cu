@@ -40,38 +40,89 @@ __device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t,
     }
 }
 
-// counts per (lag, pair, template), and the histograms that place the staging windows
-__global__ void __launch_bounds__(256) k_tap_count(TapArgs a)
+#define TAP_CACHE 4096   // walked times of one template cached in shared memory (time, L sample)
+
+// the walked times of template i and their L samples, in shared memory when they fit
+struct WalkCache {
+    int *t;
+    float2 *l;
+    int *flag;
+    bool on;
+};
+
+__device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 *L, WalkCache &wc)
+{
+    if (!wc.on) return;
+    for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
+        int t, flag;
+        tap_time(a, i, k, t, flag);
+        wc.t[k] = t;
+        wc.flag[k] = flag;
+        wc.l[k] = L[t];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void walk_at(const TapArgs &a, int i, const float2 *L, const WalkCache &wc, int k, int &t,
+                                        int &flag, float2 &l)
+{
+    if (wc.on) {
+        t = wc.t[k];
+        flag = wc.flag[k];
+        l = wc.l[k];
+    } else {
+        tap_time(a, i, k, t, flag);
+        l = L[t];
+    }
+}
+
+// counts per (lag, pair, template), and the histograms that place the staging windows: one
+// block per template walks every lag of the chunk; the histograms are flushed once per block
+__global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
 {
     __shared__ int c[EXM_NPAIR];
     __shared__ int hd[256];
     __shared__ int hb[EXM_HB_N];
-    const int i = blockIdx.x, rl = blockIdx.y;
-    const bool do_hb = a.want_hb && rl == 0;
-    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) c[q] = 0;
+    extern __shared__ unsigned char wsm[];
+    const int i = blockIdx.x;
+    const bool do_hb = a.want_hb;
     for (int q = threadIdx.x; q < 256; q += blockDim.x) hd[q] = 0;
     if (do_hb)
         for (int q = threadIdx.x; q < EXM_HB_N; q += blockDim.x) hb[q] = 0;
-    __syncthreads();
     const int nt = a.g.nt;
-    const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
     const double boff = a.boff[i];
-    for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
-        int t, flag;
-        tap_time(a, i, k, t, flag);
-        int i1 = t + tau0;
-        if (i1 >= nt) i1 -= nt;
-        int p, ib, d0;
-        float w, fb, fd;
-        exm_tap_geom(L[t], H[i1], boff, a.g, p, w, ib, fb, d0, fd);
-        atomicAdd(&c[p], 1);
-        atomicAdd(&hd[d0], 1);
-        if (do_hb) atomicAdd(&hb[ib - EXM_HB_LO], 1);
+    WalkCache wc;
+    wc.on = a.nwalk <= TAP_CACHE;
+    wc.l = (float2 *)wsm;
+    wc.t = (int *)(wc.l + TAP_CACHE);
+    wc.flag = wc.t + TAP_CACHE;
+    load_walk(a, i, L, wc);
+    for (int rl = 0; rl < rc; ++rl) {
+        for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) c[q] = 0;
+        __syncthreads();
+        const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
+        for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
+            int t, flag;
+            float2 l;
+            walk_at(a, i, L, wc, k, t, flag, l);
+            int i1 = t + tau0;
+            if (i1 >= nt) i1 -= nt;
+            int p, ib, d0;
+            float w, fb, fd;
+            exm_tap_geom(l, H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+            // warp-aggregated increments: one atomic per distinct bin in the warp
+            const unsigned pm = __match_any_sync(__activemask(), p);
+            if ((threadIdx.x & 31) == __ffs(pm) - 1) atomicAdd(&c[p], __popc(pm));
+            const unsigned dm = __match_any_sync(__activemask(), d0);
+            if ((threadIdx.x & 31) == __ffs(dm) - 1) atomicAdd(&hd[d0], __popc(dm));
+            if (do_hb && rl == 0) atomicAdd(&hb[ib - EXM_HB_LO], 1);
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x)
+            a.cnt[((long long)rl * EXM_NPAIR + q) * (a.nmc + 1) + i] = c[q];
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x)
-        a.cnt[((long long)rl * EXM_NPAIR + q) * (a.nmc + 1) + i] = c[q];
     for (int q = threadIdx.x; q < 256; q += blockDim.x)
         if (hd[q]) atomicAdd(&a.hist_d[q], hd[q]);
     if (do_hb)
@@ -122,60 +173,72 @@ __global__ void __launch_bounds__(1024) k_tap_scan(int *cnt, int nmc)
         c[p * (nmc + 1) + nmc] = (p + 1 < EXM_NPAIR) ? c[(p + 1) * (nmc + 1)] : carry;
 }
 
-// descriptors, stably scattered to their (lag, pair, template) runs
-__global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a)
+// descriptors, stably scattered to their (lag, pair, template) runs: one block per template,
+// every lag of the chunk in turn
+__global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
 {
     __shared__ int wcnt[8][EXM_NPAIR];
     __shared__ int base[EXM_NPAIR];
-    const int i = blockIdx.x, rl = blockIdx.y;
+    extern __shared__ unsigned char wsm[];
+    const int i = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nt = a.g.nt;
-    const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
     const double boff = a.boff[i];
-    const int *off = a.cnt + (long long)rl * EXM_NPAIR * (a.nmc + 1);
-    uint4 *desc = a.desc + (long long)rl * a.per_lag;
-    int32_t *tside = a.tside + (long long)rl * a.per_lag;
-    for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) base[q] = off[q * (a.nmc + 1) + i];
+    WalkCache wc;
+    wc.on = a.nwalk <= TAP_CACHE;
+    wc.l = (float2 *)wsm;
+    wc.t = (int *)(wc.l + TAP_CACHE);
+    wc.flag = wc.t + TAP_CACHE;
+    load_walk(a, i, L, wc);
     const unsigned lt = (1u << lane) - 1u;
-    for (int k0 = 0; k0 < a.nwalk; k0 += blockDim.x) {
-        for (int q = threadIdx.x; q < 8 * EXM_NPAIR; q += blockDim.x) (&wcnt[0][0])[q] = 0;
+    for (int rl = 0; rl < rc; ++rl) {
+        const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
+        const int *off = a.cnt + (long long)rl * EXM_NPAIR * (a.nmc + 1);
+        uint4 *desc = a.desc + (long long)rl * a.per_lag;
+        int32_t *tside = a.tside + (long long)rl * a.per_lag;
         __syncthreads();
-        const int k = k0 + threadIdx.x;
-        int p = -1, t = 0, flag = 0, ib = 0, d0 = 0;
-        float w = 0.f, fb = 0.f, fd = 0.f;
-        if (k < a.nwalk) {
-            tap_time(a, i, k, t, flag);
-            int i1 = t + tau0;
-            if (i1 >= nt) i1 -= nt;
-            exm_tap_geom(L[t], H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+        for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) base[q] = off[q * (a.nmc + 1) + i];
+        for (int k0 = 0; k0 < a.nwalk; k0 += blockDim.x) {
+            for (int q = threadIdx.x; q < 8 * EXM_NPAIR; q += blockDim.x) (&wcnt[0][0])[q] = 0;
+            __syncthreads();
+            const int k = k0 + threadIdx.x;
+            int p = -1, t = 0, flag = 0, ib = 0, d0 = 0;
+            float w = 0.f, fb = 0.f, fd = 0.f;
+            if (k < a.nwalk) {
+                float2 l;
+                walk_at(a, i, L, wc, k, t, flag, l);
+                int i1 = t + tau0;
+                if (i1 >= nt) i1 -= nt;
+                exm_tap_geom(l, H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+            }
+            const unsigned peers = __match_any_sync(0xffffffffu, p);
+            const int rk = __popc(peers & lt);
+            if (p >= 0 && rk == 0) wcnt[warp][p] = __popc(peers);
+            __syncthreads();
+            int pos = 0;
+            if (p >= 0) {
+                int pre = 0;
+                for (int ww = 0; ww < warp; ++ww) pre += wcnt[ww][p];
+                pos = base[p] + pre + rk;
+            }
+            __syncthreads();
+            if (threadIdx.x < EXM_NPAIR) {
+                int s2 = 0;
+                for (int ww = 0; ww < 8; ++ww) s2 += wcnt[ww][threadIdx.x];
+                base[threadIdx.x] += s2;
+            }
+            if (p >= 0 && pos >= 0 && pos < a.per_lag) {
+                uint4 d;
+                d.x = __float_as_uint(fb);
+                d.y = __float_as_uint(fd);
+                d.z = __float_as_uint(w) | ((unsigned)flag << 31);
+                d.w = ((unsigned)i << 19) | ((unsigned)d0 << 11) | ((unsigned)ib & 0x7FFu);
+                desc[pos] = d;
+                tside[pos] = t;
+            }
+            __syncthreads();
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, p);
-        const int rk = __popc(peers & lt);
-        if (p >= 0 && rk == 0) wcnt[warp][p] = __popc(peers);
-        __syncthreads();
-        int pos = 0;
-        if (p >= 0) {
-            int pre = 0;
-            for (int ww = 0; ww < warp; ++ww) pre += wcnt[ww][p];
-            pos = base[p] + pre + rk;
-        }
-        __syncthreads();
-        if (threadIdx.x < EXM_NPAIR) {
-            int s = 0;
-            for (int ww = 0; ww < 8; ++ww) s += wcnt[ww][threadIdx.x];
-            base[threadIdx.x] += s;
-        }
-        if (p >= 0 && pos >= 0 && pos < a.per_lag) {
-            uint4 d;
-            d.x = __float_as_uint(fb);
-            d.y = __float_as_uint(fd);
-            d.z = __float_as_uint(w) | ((unsigned)flag << 31);
-            d.w = ((unsigned)i << 19) | ((unsigned)d0 << 11) | ((unsigned)ib & 0x7FFu);
-            desc[pos] = d;
-            tside[pos] = t;
-        }
-        __syncthreads();
     }
 }
 
@@ -241,10 +304,12 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     a.per_lag = (long long)ci.nmc * ci.nwalk;
     if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
     EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
-    dim3 grid(ci.nmc, rc);
-    k_tap_count<<<grid, 256, 0, ctx->stream>>>(a);
+    const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int)) : 0;
+    EXM_CUDA(cudaFuncSetAttribute(k_tap_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    EXM_CUDA(cudaFuncSetAttribute(k_tap_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    k_tap_count<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_tap_scan<<<rc, 1024, 0, ctx->stream>>>(a.cnt, ci.nmc);
-    k_tap_scatter<<<grid, 256, 0, ctx->stream>>>(a);
+    k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           (int *)sl.win.p);
     EXM_CUDA(cudaGetLastError());
