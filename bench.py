@@ -153,8 +153,8 @@ def measured_peaks():
 
 
 def profiled_traffic():
-    """dram bytes per plane-gather launch of this workload, from the committed ncu summary"""
-    path = os.path.join(ROOT, "profiles", "k_gather_planes_prod.md")
+    """dram bytes per plane-gather launch of the full workload, from the committed ncu launch list"""
+    path = os.path.join(ROOT, "profiles", "launches_pe_intrinsic_prod.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -219,6 +219,51 @@ def run_reference(args):
 
 # ----------------------------------------------------------------------------- B200 arm
 
+def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
+    """the same segments served by exmarg_b200.serve.Server: child contexts sharing the resident
+    tables, two banks (all 2048 templates and the first 1024), graph replay on the workers.
+    'batched': every request queued at once (segments in flight together); 'poisson': arrivals at
+    80 % of the plain path's capacity.  Served ln Lambda of the 2048-template bank is compared
+    bitwise with the plain call's."""
+    import exmarg_b200 as eb
+    from exmarg_b200.serve import Request, Server, latency_stats
+    half = eb.MassBank(rows[:1024, 0], rows[:1024, 1], rows[:1024, 2], seg, "b200", device_index=local)
+    banks = {"bank2048": bank, "bank1024": half}
+    first = args.warmup
+    n_req = args.serve_requests
+    n_rows = len(plain)
+    mix = [("bank2048" if i % 3 else "bank1024", first + (i % n_rows)) for i in range(n_req)]
+    out = {}
+    srv = Server(store, banks, device=local, max_workers=args.serve_workers, graph=True)
+    try:
+        # warm-up with the same mix (workers per bank as the mix needs them: allocation, FFT plans,
+        # graph capture happen here)
+        srv.serve([Request(-1 - i, k, seg, row=0) for i, (k, _) in enumerate(mix[:4 * args.serve_workers])])
+        for leg in ("batched", "poisson"):
+            reqs = [Request(i, k, seg, row=r) for i, (k, r) in enumerate(mix)]
+            if leg == "batched":
+                arrivals = None
+            else:
+                rate = 0.8 * capacity
+                arrivals = np.cumsum(np.random.default_rng(7).exponential(1.0 / rate, n_req)) - 1.0 / rate
+            done = srv.serve(reqs, arrivals)
+            same = True
+            for r in done:
+                lnl, _ = r.future.result()
+                if r.key == "bank2048":
+                    same &= bool(np.array_equal(lnl, plain[r.row - first]["ln_lambda"][0]))
+            st = latency_stats(done)
+            d = {"requests": n_req, "workers": args.serve_workers, "segments_per_s": st["segments_per_s"],
+                 "latency_ms_p50": st["p50_ms"], "latency_ms_p99": st["p99_ms"],
+                 "identical_to_plain": same, "banks": "2048 and 1024 templates (2:1)"}
+            if leg == "poisson":
+                d["offered_per_s"] = 0.8 * capacity
+            out[leg] = d
+    finally:
+        srv.close()
+    return out
+
+
 def run_b200(args):
     rank, world, local = dist_env()
     import exmarg_b200 as eb
@@ -247,7 +292,10 @@ def run_b200(args):
     for i in range(args.warmup):
         eb.pe_intrinsic(seg, bank, store, rows=[i])
     tune = None
-    if not args.no_tune:
+    if args.gather_cfg >= 0:
+        ctx.set_gather_cfg(args.gather_cfg)
+        tune = {"chosen": args.gather_cfg, "forced": True}
+    elif not args.no_tune:
         best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
         tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:5]],
                 "shapes": ["16w x4", "16w x2", "24w x2", "32w x2", "32w x1"]}
@@ -280,7 +328,8 @@ def run_b200(args):
     bytes_per_launch = (32.0 * tm["node_taps"] + 16.0 * tm["tlw_taps"]) / max(launches, 1)
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / (g_ms / 1000.0) / 1e9
-    traffic = profiled_traffic()
+    full = args.templates == N_TEMPLATES and args.nodes == 53 and args.lags == 87
+    traffic = profiled_traffic() if full else None
     line = {"metric": METRIC, "value": value, "unit": "segments/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
@@ -297,6 +346,8 @@ def run_b200(args):
                          "node_taps_per_launch": tm["node_taps"] / max(launches, 1),
                          "dram_gbs": (traffic / (g_ms / 1000.0) / 1e9) if traffic else None},
             "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -334,6 +385,9 @@ def main():
     ap.add_argument("--templates", type=int, default=N_TEMPLATES, help="bank size (reduced profiling cases)")
     ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
     ap.add_argument("--lags", type=int, default=87, help="table lags (reduced profiling cases; odd)")
+    ap.add_argument("--gather-cfg", type=int, default=-1, help="force a gather launch shape (no autotuning)")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
+    ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -18,7 +18,7 @@ DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_rng_integers", "exm_ctx_timing", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg")
@@ -41,9 +41,12 @@ def load():
     P, I, D, Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
     sig = {
         "exm_version": ([], I),
+        "exm_device_memory": ([I, ctypes.POINTER(Z), ctypes.POINTER(Z)], I),
         "exm_rng_integers": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int64, P], I),
         "exm_ctx_create": ([I, Z, ctypes.POINTER(P)], I),
         "exm_ctx_destroy": ([P], None),
+        "exm_ctx_create_sharing": ([P, Z, ctypes.POINTER(P)], I),
+        "exm_ctx_set_graph": ([P, I], I),
         "exm_last_error": ([P], ctypes.c_char_p),
         "exm_ctx_bytes": ([P], Z),
         "exm_ctx_timing": ([P, I, P], I),
@@ -81,6 +84,15 @@ def rng_integers(seed, high, count):
     return out
 
 
+def device_memory(device=0):
+    """(free, total) bytes of a CUDA device"""
+    f, t = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = load().exm_device_memory(int(device), ctypes.byref(f), ctypes.byref(t))
+    if rc != EXM_OK:
+        _raise(rc, "cannot query CUDA device %d" % device)
+    return f.value, t.value
+
+
 def _raise(code, msg):
     if code == EXM_ERR_ARG:
         raise ValueError(msg)
@@ -92,17 +104,29 @@ def _raise(code, msg):
 class Context:
     """one device context of libexmarg_b200 (tables, bank, workspaces, one stream)"""
 
-    def __init__(self, device=0, hbm_budget=0):
+    def __init__(self, device=0, hbm_budget=0, share_store_of=None):
         self.lib = load()
         h = ctypes.c_void_p()
-        rc = self.lib.exm_ctx_create(int(device), int(hbm_budget), ctypes.byref(h))
-        if rc != EXM_OK:
-            _raise(rc, "cannot open CUDA device %d for libexmarg_b200 (status %d)" % (device, rc))
+        if share_store_of is not None:
+            rc = self.lib.exm_ctx_create_sharing(share_store_of.h, int(hbm_budget), ctypes.byref(h))
+            if rc != EXM_OK:
+                _raise(rc, share_store_of.lib.exm_last_error(share_store_of.h).decode())
+            device = share_store_of.device
+            self.parent = share_store_of            # keeps the store's owner alive
+        else:
+            rc = self.lib.exm_ctx_create(int(device), int(hbm_budget), ctypes.byref(h))
+            if rc != EXM_OK:
+                _raise(rc, "cannot open CUDA device %d for libexmarg_b200 (status %d)" % (device, rc))
         self.h = h
         self.device = device
-        self.store_token = None
+        self.store_token = share_store_of.store_token if share_store_of is not None else None
         self.bank_token = None
         self.prep_token = None
+        self.nm = self.nfreq = self.n_time = None
+
+    def set_graph(self, enable=True):
+        """replay each segment's device work as one captured CUDA graph"""
+        self._check(self.lib.exm_ctx_set_graph(self.h, 1 if enable else 0))
 
     def close(self):
         if getattr(self, "h", None):

@@ -77,7 +77,15 @@ class MassBank:
 
     @property
     def ctx(self):
-        return _lib.context(self.device_index)
+        c = getattr(self, "_ctx", None)
+        return c if c is not None else _lib.context(self.device_index)
+
+    def clone_for(self, ctx):
+        """the same bank (host arrays shared) bound to another context, e.g. a child context"""
+        seg = dict(T=self.T, fmin=self.fmin, fmax=self.fmax, nu=self.nu)
+        b = MassBank(self.M, self.q, self.chi, seg, "b200", W=self.W, u=self.u, device_index=ctx.device)
+        b._ctx = ctx
+        return b
 
     def upload(self):
         """make this bank the context's current bank (W copied to HBM)"""

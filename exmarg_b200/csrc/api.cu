@@ -5,6 +5,8 @@
 #include <cstring>
 #include <numeric>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "pcg64.cuh"
@@ -14,7 +16,6 @@ void exm_store_generate(exm_ctx *ctx, int k, const float *M, const float *P, con
 void exm_run_node_values(exm_ctx *ctx, exm_slot &sl, double *d_lamN);
 void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,
                                 const double *d_p, int n_dens);
-void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S);
 void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
 
 // ------------------------------------------------------------------ memory
@@ -35,6 +36,7 @@ void exm_alloc(exm_ctx *ctx, dbuf &b, size_t bytes)
     b.p = p;
     b.bytes = bytes;
     ctx->used += bytes;
+    ctx->alloc_gen++;
 }
 
 void exm_free(exm_ctx *ctx, dbuf &b)
@@ -42,6 +44,7 @@ void exm_free(exm_ctx *ctx, dbuf &b)
     if (b.p) {
         cudaFree(b.p);
         ctx->used -= b.bytes;
+        ctx->alloc_gen++;
     }
     b.p = nullptr;
     b.bytes = 0;
@@ -166,6 +169,16 @@ extern "C" int exm_ctx_timing(exm_ctx *ctx, int enable, double *out)
 
 extern "C" int exm_version(void) { return 10000; }
 
+extern "C" int exm_device_memory(int device, size_t *free_bytes, size_t *total_bytes)
+{
+    if (!free_bytes || !total_bytes) return EXM_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(free_bytes, total_bytes) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return EXM_ERR_CUDA;
+    }
+    return EXM_OK;
+}
+
 extern "C" int exm_rng_integers(uint64_t seed, uint32_t high, int64_t count, int64_t *out)
 {
     if (high < 1 || count < 0 || (count > 0 && !out)) return EXM_ERR_ARG;
@@ -224,12 +237,81 @@ extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
     return EXM_OK;
 }
 
-extern "C" void exm_ctx_destroy(exm_ctx *ctx)
+extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ctx **out)
 {
-    if (!ctx) return;
+    if (!parent || !out) return EXM_ERR_ARG;
+    *out = nullptr;
+    if (parent->store_borrowed) parent = parent->parent;   // share the owner's store, not a child's
+    if (!parent->store_ok) {
+        parent->err = "the parent context has no complete store to share";
+        return EXM_ERR_STATE;
+    }
+    exm_ctx *ctx = new exm_ctx();
+    try {
+        EXM_CUDA(cudaSetDevice(parent->dev));
+        ctx->dev = parent->dev;
+        EXM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->sm_count = parent->sm_count;
+        ctx->smem_optin = parent->smem_optin;
+        size_t fr = 0, tot = 0;
+        EXM_CUDA(cudaMemGetInfo(&fr, &tot));
+        ctx->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+        ctx->store_ok = true;
+        ctx->store_borrowed = true;
+        ctx->nn = parent->nn;
+        ctx->ntau = parent->ntau;
+        ctx->nphif = parent->nphif;
+        ctx->nb = parent->nb;
+        ctx->nd = parent->nd;
+        ctx->ndp = parent->ndp;
+        ctx->dtype = parent->dtype;
+        ctx->beta0 = parent->beta0;
+        ctx->dbeta = parent->dbeta;
+        ctx->delta0 = parent->delta0;
+        ctx->ddelta = parent->ddelta;
+        ctx->tau = parent->tau;
+        ctx->s = parent->s;
+        ctx->alo = parent->alo;
+        ctx->ahi = parent->ahi;
+        ctx->node_set = parent->node_set;
+        ctx->T.p = parent->T.p;            // borrowed: not counted, not freed
+        ctx->tstride = parent->tstride;
+        ctx->d_tau.p = parent->d_tau.p;
+        ctx->tmap = parent->tmap;
+        ctx->tmap_ok = parent->tmap_ok;
+        ctx->gather_cfg = parent->gather_cfg;
+        exm_ensure(ctx, ctx->d_stats, 4 * sizeof(unsigned long long));
+        EXM_CUDA(cudaMemset(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long)));
+    } catch (const exm_error &e) {
+        parent->err = e.msg;
+        exm_free(ctx, ctx->d_stats);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return e.code;
+    }
+    ctx->parent = parent;
+    parent->n_children.fetch_add(1);
+    *out = ctx;
+    return EXM_OK;
+}
+
+extern "C" int exm_ctx_set_graph(exm_ctx *ctx, int enable)
+{
+    if (!ctx) return EXM_ERR_ARG;
+    ctx->use_graph = enable != 0;
+    return EXM_OK;
+}
+
+static void ctx_free(exm_ctx *ctx)
+{
     cudaSetDevice(ctx->dev);
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->plan) cufftDestroy(ctx->plan);
+    if (ctx->store_borrowed) {   // the parent owns the tables
+        ctx->T = dbuf();
+        ctx->d_tau = dbuf();
+    }
     free_slot(ctx, ctx->slot);
     for (auto &e : ctx->ev_pool) {
         cudaEventDestroy(e.first);
@@ -242,6 +324,41 @@ extern "C" void exm_ctx_destroy(exm_ctx *ctx)
     delete ctx;
 }
 
+static std::mutex g_attr_mu;
+static std::vector<std::pair<int, const void *>> g_attr_done;   // (device, kernel) raised to the opt-in limit
+
+void exm_allow_smem(exm_ctx *ctx, const void *func, size_t smem)
+{
+    if (smem > ctx->smem_optin)
+        EXM_THROW(EXM_ERR_ARG, "a kernel needs " + std::to_string(smem) + " B of shared memory, above the device's " +
+                                   std::to_string(ctx->smem_optin) + " B");
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    const std::pair<int, const void *> key(ctx->dev, func);
+    if (std::find(g_attr_done.begin(), g_attr_done.end(), key) != g_attr_done.end()) return;
+    EXM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
+    g_attr_done.push_back(key);
+}
+
+static std::mutex g_destroy_mu;   // orders a parent's deferred free against its children's destroys
+
+// A parent destroyed while child contexts still borrow its tables keeps them until the last
+// child is destroyed (its other calls are the caller's to stop).
+extern "C" void exm_ctx_destroy(exm_ctx *ctx)
+{
+    if (!ctx) return;
+    exm_ctx *parent = ctx->parent, *free_parent = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_destroy_mu);
+        if (!parent && ctx->n_children.load() > 0) {
+            ctx->destroy_pending = true;
+            return;
+        }
+        if (parent && parent->n_children.fetch_sub(1) == 1 && parent->destroy_pending) free_parent = parent;
+    }
+    ctx_free(ctx);
+    if (free_parent) ctx_free(free_parent);
+}
+
 extern "C" const char *exm_last_error(const exm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 extern "C" size_t exm_ctx_bytes(const exm_ctx *ctx) { return ctx ? ctx->used : 0; }
@@ -252,6 +369,8 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
                               const int64_t *tau_idx, double beta0, double dbeta, double delta0, double ddelta)
 {
     API_BEGIN(ctx)
+    REQUIRE(!ctx->store_borrowed, EXM_ERR_STATE, "this context borrows its parent's store");
+    REQUIRE(ctx->n_children.load() == 0, EXM_ERR_STATE, "child contexts borrow this store: destroy them first");
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(n_nodes >= 1 && n_nodes <= EXM_MAX_NODES, EXM_ERR_ARG, "n_nodes must be 1..64");
     REQUIRE(ntau >= 1 && tau_idx, EXM_ERR_ARG, "need at least one lag");
@@ -309,6 +428,8 @@ static void set_node_meta(exm_ctx *ctx, int k, double s, double alo, double ahi)
 extern "C" int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *T)
 {
     API_BEGIN(ctx)
+    REQUIRE(!ctx->store_borrowed, EXM_ERR_STATE, "this context borrows its parent's store");
+    REQUIRE(ctx->n_children.load() == 0, EXM_ERR_STATE, "child contexts borrow this store: destroy them first");
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(T, EXM_ERR_ARG, "null table");
     set_node_meta(ctx, k, s, alpha_lo, alpha_hi);
@@ -324,6 +445,8 @@ extern "C" int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alp
                                        const float *P, const float *Q, float S, uint32_t seed)
 {
     API_BEGIN(ctx)
+    REQUIRE(!ctx->store_borrowed, EXM_ERR_STATE, "this context borrows its parent's store");
+    REQUIRE(ctx->n_children.load() == 0, EXM_ERR_STATE, "child contexts borrow this store: destroy them first");
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(M && P && Q, EXM_ERR_ARG, "null generator factors");
     set_node_meta(ctx, k, s, alpha_lo, alpha_hi);
@@ -575,8 +698,8 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
     exm_ensure(ctx, sl.lnl, (size_t)ctx->nm * sizeof(double));
     exm_ensure(ctx, sl.lnb, sizeof(double));
     exm_ensure(ctx, sl.dev_err, sizeof(unsigned));
-    exm_ensure(ctx, sl.din, 6 * nf * sizeof(double) + 2 * nf * sizeof(float2));
-    const size_t hin = 6 * nf * sizeof(double);
+    exm_ensure(ctx, sl.din, 6 * nf * sizeof(double) + 2 * nf * sizeof(float2) + 4 * sizeof(uint64_t));
+    const size_t hin = 6 * nf * sizeof(double) + 4 * sizeof(uint64_t);
     if (!sl.hostin.p || sl.hostin.bytes < hin) {
         if (sl.hostin.p) cudaFreeHost(sl.hostin.p);
         sl.hostin.p = nullptr;
@@ -585,8 +708,9 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
     }
 }
 
-static void stage_input(exm_ctx *ctx, exm_slot &sl, const double *dH, const double *dL, const double *s2H,
-                        const double *s2L)
+// the segment's data and the PCG64 state of its seed into the pinned staging buffer
+static void stage_host(exm_ctx *ctx, exm_slot &sl, const double *dH, const double *dL, const double *s2H,
+                       const double *s2L, uint64_t seed)
 {
     const size_t nf = ctx->nfreq;
     double *h = (double *)sl.hostin.p;
@@ -594,7 +718,27 @@ static void stage_input(exm_ctx *ctx, exm_slot &sl, const double *dH, const doub
     memcpy(h + 2 * nf, dL, 2 * nf * sizeof(double));
     memcpy(h + 4 * nf, s2H, nf * sizeof(double));
     memcpy(h + 5 * nf, s2L, nf * sizeof(double));
-    EXM_CUDA(cudaMemcpyAsync(sl.din.p, h, 6 * nf * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    exm_pcg_words(seed, (uint64_t *)(h + 6 * nf));
+}
+
+// the staged input to the device (a stream operation: part of a captured graph)
+static void copy_input(exm_ctx *ctx, exm_slot &sl)
+{
+    const size_t nf = ctx->nfreq;
+    EXM_CUDA(cudaMemcpyAsync(sl.din.p, sl.hostin.p, 6 * nf * sizeof(double) + 4 * sizeof(uint64_t),
+                             cudaMemcpyHostToDevice, ctx->stream));
+}
+
+static const uint64_t *state_words(exm_ctx *ctx, exm_slot &sl)
+{
+    return (const uint64_t *)((const double *)sl.din.p + 6 * (size_t)ctx->nfreq);
+}
+
+static void stage_input(exm_ctx *ctx, exm_slot &sl, const double *dH, const double *dL, const double *s2H,
+                        const double *s2L, uint64_t seed = 0)
+{
+    stage_host(ctx, sl, dH, dL, s2H, s2L, seed);
+    copy_input(ctx, sl);
 }
 
 static void check_dev_err(exm_ctx *ctx, exm_slot &sl)
@@ -608,13 +752,13 @@ static void check_dev_err(exm_ctx *ctx, exm_slot &sl)
 }
 
 // everything of one segment from the staged input to lnl / lnb on the device
-static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs, uint64_t seed)
+static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
 {
     const int tt = exm_tim_begin(ctx, 0);
     EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
     if (rs.K > 0) {
         const int h = exm_tim_begin(ctx, 2);
-        exm_run_pcg(ctx, sl, seed, rs.K, rs.S);
+        exm_run_pcg(ctx, sl, state_words(ctx, sl), rs.K, rs.S);
         exm_tim_end(ctx, h);
     }
     for (int m_base = 0; m_base < ctx->nm; m_base += rs.nmc_max) {
@@ -648,6 +792,61 @@ static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs, uint64_t
     ctx->segments += 1;
 }
 
+// the whole per-segment device sequence (input copy included) as one CUDA graph, captured on
+// first use for the current shape and buffers and replayed for every later segment
+static void run_segment_graph(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
+{
+    const long long key[6] = {ctx->nm, ctx->nt, rs.K, rs.S, ctx->gather_cfg, ctx->alloc_gen};
+    if (!ctx->graph_exec || memcmp(key, ctx->graph_key, sizeof(key)) != 0) {
+        if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        exm_fft_plan(ctx, 2 * ctx->nm);   // plans and work areas exist before the capture
+        const long long gen0 = ctx->alloc_gen;
+        const bool tim = ctx->tim_on;
+        const double taps0 = ctx->node_taps, tlw0 = ctx->tlw, seg0 = ctx->segments;
+        const long long l0 = ctx->launches, g0 = ctx->gather_launches;
+        ctx->tim_on = false;
+        cudaGraph_t g = nullptr;
+        EXM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            copy_input(ctx, sl);
+            run_segment(ctx, sl, rs);
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            ctx->tim_on = tim;
+            throw;
+        }
+        EXM_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+        ctx->tim_on = tim;
+        if (ctx->alloc_gen != gen0) {   // something was allocated while capturing: buffers not stable
+            cudaGraphDestroy(g);
+            EXM_THROW(EXM_ERR_STATE, "workspace changed while capturing the segment graph");
+        }
+        cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        EXM_CUDA(e);
+        ctx->graph_node_taps = ctx->node_taps - taps0;
+        ctx->graph_tlw = ctx->tlw - tlw0;
+        ctx->graph_launches = ctx->launches - l0;
+        ctx->graph_gathers = ctx->gather_launches - g0;
+        ctx->node_taps = taps0;   // counted per replay below
+        ctx->tlw = tlw0;
+        ctx->segments = seg0;
+        ctx->launches = l0;
+        ctx->gather_launches = g0;
+        memcpy(ctx->graph_key, key, sizeof(key));
+    }
+    const int h = exm_tim_begin(ctx, 0);
+    EXM_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    exm_tim_end(ctx, h);
+    ctx->node_taps += ctx->graph_node_taps;
+    ctx->tlw += ctx->graph_tlw;
+    ctx->launches += ctx->graph_launches;
+    ctx->gather_launches += ctx->graph_gathers;
+    ctx->segments += 1;
+}
+
 extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const double *d_L, const double *sig2_H,
                                 const double *sig2_L, const int64_t *seeds, int n_loud, int n_random,
                                 double *ln_lambda, double *ln_b)
@@ -662,10 +861,17 @@ extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, cons
     ensure_slot(ctx, sl, rs);
     std::vector<double> lnl(ctx->nm);
     const size_t nf = ctx->nfreq;
+    const bool graph = ctx->use_graph && ctx->nm <= rs.nmc_max && rs.rc >= ctx->ntau;
     for (int e = 0; e < n_seg; ++e) {
         REQUIRE(rs.K == 0 || seeds[e] >= 0, EXM_ERR_ARG, "seed must be non-negative");
-        stage_input(ctx, sl, d_H + (size_t)e * 2 * nf, d_L + (size_t)e * 2 * nf, sig2_H, sig2_L);
-        run_segment(ctx, sl, rs, rs.K > 0 ? (uint64_t)seeds[e] : 0);
+        const uint64_t seed = rs.K > 0 ? (uint64_t)seeds[e] : 0;
+        if (graph) {
+            stage_host(ctx, sl, d_H + (size_t)e * 2 * nf, d_L + (size_t)e * 2 * nf, sig2_H, sig2_L, seed);
+            run_segment_graph(ctx, sl, rs);
+        } else {
+            stage_input(ctx, sl, d_H + (size_t)e * 2 * nf, d_L + (size_t)e * 2 * nf, sig2_H, sig2_L, seed);
+            run_segment(ctx, sl, rs);
+        }
         EXM_CUDA(cudaMemcpyAsync(lnl.data(), sl.lnl.p, sizeof(double) * ctx->nm, cudaMemcpyDeviceToHost, ctx->stream));
         EXM_CUDA(cudaMemcpyAsync(ln_b + e, sl.lnb.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         check_dev_err(ctx, sl);
@@ -811,7 +1017,11 @@ extern "C" int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_ra
     RunShape rs = stage_shape(ctx, n_loud, n_random);
     exm_slot &sl = ctx->slot;
     ensure_slot(ctx, sl, rs);
-    exm_run_pcg(ctx, sl, (uint64_t)seed, rs.K, rs.S);
+    uint64_t *w = (uint64_t *)((double *)sl.hostin.p + 6 * (size_t)ctx->nfreq);
+    exm_pcg_words((uint64_t)seed, w);
+    EXM_CUDA(cudaMemcpyAsync((void *)state_words(ctx, sl), w, 4 * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    exm_run_pcg(ctx, sl, state_words(ctx, sl), rs.K, rs.S);
     exm_run_topk(ctx, sl, ctx->nm, (const int *)ctx->d_order.p, rs.K, rs.S);
     EXM_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->times_ok = true;

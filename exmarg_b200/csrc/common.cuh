@@ -7,6 +7,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -81,8 +82,11 @@ struct exm_ctx {
     int sm_count = 148;
     size_t smem_optin = 0;
 
-    // store
-    bool store_ok = false;
+    // store (a child context borrows its parent's: it neither fills nor frees it)
+    bool store_ok = false, store_borrowed = false;
+    exm_ctx *parent = nullptr;              // the context whose store this one borrows
+    std::atomic<int> n_children{0};         // child contexts borrowing this context's store
+    bool destroy_pending = false;           // destroyed while children were alive: freed with the last one
     int nn = 0, ntau = 0, nphif = 0, nb = 0, nd = 0, ndp = 0, dtype = 0;
     double beta0 = 0, dbeta = 0, delta0 = 0, ddelta = 0;
     std::vector<int64_t> tau;
@@ -126,6 +130,14 @@ struct exm_ctx {
     int plan_batch = 0, plan_n = 0;
     dbuf fftwork;
 
+    // CUDA graph of the per-segment device work (captured on first use for a shape, then replayed)
+    bool use_graph = false;
+    long long alloc_gen = 0;   // bumped by every allocation or free: a captured graph's buffers moved
+    cudaGraphExec_t graph_exec = nullptr;
+    long long graph_key[6] = {0, 0, 0, 0, 0, 0};
+    double graph_node_taps = 0, graph_tlw = 0;
+    long long graph_launches = 0, graph_gathers = 0;
+
     // CUDA-event timing of the pipeline stages on the context's stream
     bool tim_on = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
@@ -152,3 +164,10 @@ void exm_tim_collect(exm_ctx *ctx);   // after a stream synchronisation
 void exm_alloc(exm_ctx *ctx, dbuf &b, size_t bytes);
 void exm_free(exm_ctx *ctx, dbuf &b);
 void exm_ensure(exm_ctx *ctx, dbuf &b, size_t bytes);   // grow-only
+
+// Let `func` take up to the device's opt-in shared memory per block (cudaFuncAttribute-
+// MaxDynamicSharedMemorySize).  The attribute belongs to the function on the device, not to a
+// context or stream, so it is raised to the largest value once per device and never lowered:
+// contexts on several host threads launching the same kernel with different sizes cannot undo
+// each other's setting.  Throws if `smem` exceeds the opt-in limit.
+void exm_allow_smem(exm_ctx *ctx, const void *func, size_t smem);

@@ -59,7 +59,7 @@ void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm)
 {
     const int nt = ctx->nt, nf = ctx->nfreq;
     float2 *traj = (float2 *)sl.traj.p;
-    float2 *w = (float2 *)((char *)sl.din.p + (size_t)6 * nf * sizeof(double));
+    float2 *w = (float2 *)((char *)sl.din.p + (size_t)6 * nf * sizeof(double) + 4 * sizeof(uint64_t));
     k_weights<<<(2 * nf + 255) / 256, 256, 0, ctx->stream>>>((const double *)sl.din.p, nf, w);
     const long long total = 2LL * nm * nt;
     double2 *z = (double2 *)sl.fft.p;

@@ -573,7 +573,7 @@ static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs
 template <int NW, int GRP>
 static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
 {
-    EXM_CUDA(cudaFuncSetAttribute(k_gather_planes<NW, GRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP>, smem);
     k_gather_planes<NW, GRP><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
 }
 

@@ -106,7 +106,8 @@ __device__ __forceinline__ double exm_tap_fp64<float>(float2 l, float2 h, double
 
 void exm_fft_plan(exm_ctx *ctx, int batch);
 void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm);
-void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S);
+void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, const uint64_t *d_state, int K, int S);
+void exm_pcg_words(uint64_t seed, uint64_t *w);
 void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
 
 struct ChunkInfo {

@@ -50,15 +50,16 @@ __global__ void __launch_bounds__(256) k_scores(const float2 *__restrict__ trajH
 }
 
 // the stream of numpy's bounded integers: 64 draws of 32 bits per thread, rejections listed
-__global__ void k_pcg_draws(uint64_t st_hi, uint64_t st_lo, uint64_t inc_hi, uint64_t inc_lo, long long n_draws,
-                            uint32_t range, uint32_t thr, uint32_t *__restrict__ raw, int *__restrict__ rej)
+// st = {state hi, state lo, inc hi, inc lo} in device memory (staged with the segment's data)
+__global__ void k_pcg_draws(const uint64_t *__restrict__ st, long long n_draws, uint32_t range, uint32_t thr,
+                            uint32_t *__restrict__ raw, int *__restrict__ rej)
 {
     const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long q0 = g * 64;
     if (q0 >= n_draws) return;
     exm_pcg p;
-    p.state = ((exm_u128)st_hi << 64) | st_lo;
-    p.inc = ((exm_u128)inc_hi << 64) | inc_lo;
+    p.state = ((exm_u128)st[0] << 64) | st[1];
+    p.inc = ((exm_u128)st[2] << 64) | st[3];
     exm_pcg_advance(p, (uint64_t)(g * 32));
     for (int j = 0; j < 32; ++j) {
         exm_pcg_step(p);
@@ -286,24 +287,32 @@ static int next_pow2(int v)
     return p;
 }
 
+// the PCG64 state numpy's default_rng(seed) starts from, as {state hi, lo, inc hi, lo}
+void exm_pcg_words(uint64_t seed, uint64_t *w)
+{
+    const exm_pcg g = exm_pcg_from_seed(seed);
+    w[0] = (uint64_t)(g.state >> 64);
+    w[1] = (uint64_t)g.state;
+    w[2] = (uint64_t)(g.inc >> 64);
+    w[3] = (uint64_t)g.inc;
+}
+
 // the numpy draws of one segment for the whole bank (original template order):
-// integers(0, nt - K, size=(nm, S)) from default_rng(seed).  The raw draws use the
-// key buffer as scratch; the selection of each chunk overwrites it afterwards.
-void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, uint64_t seed, int K, int S)
+// integers(0, nt - K, size=(nm, S)) from default_rng(seed), the generator state read
+// from d_state (4 words on the device).  The raw draws use the key buffer as scratch;
+// the selection of each chunk overwrites it afterwards.
+void exm_run_pcg(exm_ctx *ctx, exm_slot &sl, const uint64_t *d_state, int K, int S)
 {
     const int nt = ctx->nt;
     const uint32_t range = (uint32_t)(nt - K);
     const uint32_t thr = (uint32_t)((1ull << 32) % range);
     const long long n_out = (long long)ctx->nm * S;
     const long long n_draws = ((n_out + EXM_MAX_REJ + 63) / 64) * 64;
-    const exm_pcg g = exm_pcg_from_seed(seed);
     int *rej = (int *)sl.rej.p;
     uint32_t *raw = (uint32_t *)sl.keys.p;
     EXM_CUDA(cudaMemsetAsync(rej, 0, sizeof(int), ctx->stream));
     const long long nthr = n_draws / 64;
-    k_pcg_draws<<<(unsigned)((nthr + 127) / 128), 128, 0, ctx->stream>>>(
-        (uint64_t)(g.state >> 64), (uint64_t)g.state, (uint64_t)(g.inc >> 64), (uint64_t)g.inc, n_draws, range, thr,
-        raw, rej);
+    k_pcg_draws<<<(unsigned)((nthr + 127) / 128), 128, 0, ctx->stream>>>(d_state, n_draws, range, thr, raw, rej);
     k_pcg_compact<<<(unsigned)((n_out + 255) / 256), 256, 0, ctx->stream>>>(raw, rej, n_out, (int32_t *)sl.picks.p);
     EXM_CUDA(cudaGetLastError());
     ctx->launches += 2;
@@ -322,8 +331,7 @@ void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk,
     }
     const int wn = lag_hi - lag_lo + 1;
     const size_t smem_s = (size_t)2 * (SCORE_TILE + wn - 1) * sizeof(float);
-    if (smem_s > 48 * 1024)
-        EXM_CUDA(cudaFuncSetAttribute(k_scores, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s));
+    if (smem_s > 48 * 1024) exm_allow_smem(ctx, (const void *)k_scores, smem_s);
     dim3 gs((nt + SCORE_TILE - 1) / SCORE_TILE, nmc);
     k_scores<<<gs, 256, smem_s, ctx->stream>>>(trajH, trajL, nt, lag_lo, lag_hi, (uint32_t *)sl.keys.p);
     EXM_CUDA(cudaGetLastError());
@@ -331,7 +339,7 @@ void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk,
     const int nwords = (nt + 31) / 32;
     const size_t smem_t = sizeof(int) * (2048 + nwords + nwords + 1 + K + Sp + 40);
     if (smem_t > ctx->smem_optin) EXM_THROW(EXM_ERR_ARG, "n_loud + n_random too large for the selection kernel");
-    EXM_CUDA(cudaFuncSetAttribute(k_topk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));
+    exm_allow_smem(ctx, (const void *)k_topk, smem_t);
     k_topk<<<nmc, 1024, smem_t, ctx->stream>>>((const uint32_t *)sl.keys.p, (const int32_t *)sl.picks.p,
                                                d_order_chunk, nt, K, S, Sp, (int32_t *)sl.sel.p);
     EXM_CUDA(cudaGetLastError());

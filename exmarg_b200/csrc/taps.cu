@@ -305,8 +305,8 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
     EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
     const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int)) : 0;
-    EXM_CUDA(cudaFuncSetAttribute(k_tap_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
-    EXM_CUDA(cudaFuncSetAttribute(k_tap_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+    exm_allow_smem(ctx, (const void *)k_tap_count, wsm);
+    exm_allow_smem(ctx, (const void *)k_tap_scatter, wsm);
     k_tap_count<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_tap_scan<<<rc, 1024, 0, ctx->stream>>>(a.cnt, ci.nmc);
     k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);

@@ -55,6 +55,19 @@ EXM_API int exm_version(void);
  * exmarg/search/pe.py:37-50 (_fit_chunk). */
 EXM_API int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out);
 EXM_API void exm_ctx_destroy(exm_ctx *ctx);
+
+/* A second context on the parent's device that borrows the parent's resident store (its
+ * tables are neither copied nor freed) and has its own stream, bank, workspace and budget:
+ * several banks and segments in flight on one GPU without a second copy of the tables.
+ * While children exist the parent refuses to change its store (EXM_ERR_STATE), and a
+ * parent destroyed before its children keeps its tables until the last child is
+ * destroyed.  No reference counterpart (one cupy device state, exmarg/search/bank.py:17-24). */
+EXM_API int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ctx **out);
+
+/* enable = 1: exm_pe_intrinsic runs each segment's device work -- input copy, filter,
+ * selection, taps, gather, epilogue -- as one CUDA graph, captured on the first segment
+ * of a shape and replayed for the rest.  No reference counterpart. */
+EXM_API int exm_ctx_set_graph(exm_ctx *ctx, int enable);
 EXM_API const char *exm_last_error(const exm_ctx *ctx);
 /* Bytes of device memory the context holds now. */
 EXM_API size_t exm_ctx_bytes(const exm_ctx *ctx);
@@ -73,6 +86,9 @@ EXM_API int exm_rng_integers(uint64_t seed, uint32_t high, int64_t count, int64_
  * that took the exact float64 path, out[12] boundary-point taps.  No reference
  * counterpart (the reference times with time.time() in its notebooks). */
 EXM_API int exm_ctx_timing(exm_ctx *ctx, int enable, double *out);
+
+/* Free and total bytes of CUDA device `device` (cudaMemGetInfo), for sizing budgets. */
+EXM_API int exm_device_memory(int device, size_t *free_bytes, size_t *total_bytes);
 
 /* ------------------------------------------------------------------ store */
 

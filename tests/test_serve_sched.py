@@ -1,0 +1,88 @@
+"""The serving scheduler (exmarg_b200.serve.Scheduler): admission by workspace budget, on the CPU."""
+
+from exmarg_b200.serve import Scheduler, workspace_bytes
+
+
+def test_admission_respects_budget_and_worker_limit():
+    cost = {"a": 40, "b": 70}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=3)
+    for i in range(4):
+        s.push(("a", i), "a")
+    s.push(("b", 0), "b")
+    got = []
+    while True:
+        g = s.admit()
+        if g[0] is None:
+            break
+        got.append(g)
+    # two 'a' workers fit (80 of 100); a third 'a' or a 'b' worker would exceed the budget
+    assert [g[0] for g in got] == [("a", 0), ("a", 1)]
+    assert s.used == 80 and s.n_workers() == 2
+    assert all(g[3] for g in got)                       # both were new workers
+    s.release(got[0][2])
+    g = s.admit()                                       # the freed 'a' worker takes the next 'a' request
+    assert g[0] == ("a", 2) and g[2] == got[0][2] and not g[3]
+    assert s.used == 80
+
+
+def test_out_of_order_admission_when_the_head_is_blocked():
+    cost = {"big": 90, "small": 10}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=4)
+    s.push("big0", "big")
+    s.push("big1", "big")
+    s.push("small0", "small")
+    a = s.admit()
+    assert a[0] == "big0"
+    b = s.admit()                                       # big1 cannot start, small0 can
+    assert b[0] == "small0"
+    assert s.admit()[0] is None
+    s.release(a[2])
+    c = s.admit()
+    assert c[0] == "big1" and c[2] == a[2]
+
+
+def test_workspace_estimate_grows_with_the_bank():
+    small = workspace_bytes(256, 16384, 53, 87, 1969, 2048)
+    big = workspace_bytes(2048, 32768, 53, 87, 3937, 2048)
+    assert 0 < small < big
+    assert 8e9 < big < 20e9
+
+
+def test_idle_workers_of_another_bank_are_evicted():
+    cost = {"a": 60, "b": 60}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=4)
+    s.push("a0", "a")
+    a = s.admit()
+    s.release(a[2])                                     # an idle 'a' worker holds 60 of 100
+    s.push("b0", "b")
+    b = s.admit()
+    assert b[0] == "b0" and b[3] and b[4] == [a[2]]     # the idle 'a' worker was evicted for it
+    assert s.used == 60
+    s.push("a1", "a")
+    assert s.admit()[0] is None                         # 'b' is busy: nothing to evict
+
+
+def test_recost_follows_live_workers():
+    cost = {"a": 50}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=4)
+    for i in range(2):
+        s.push(i, "a")
+    assert s.admit()[0] == 0 and s.admit()[0] == 1
+    assert s.used == 100
+    s.recost("a", 30, cost.__setitem__)                  # measured smaller than estimated
+    assert cost["a"] == 30 and s.used == 60
+    s.push(2, "a")
+    assert s.admit()[0] == 2 and s.used == 90
+
+
+def test_idle_worker_with_queued_work_is_kept():
+    cost = {"a": 60, "b": 60}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=4)
+    s.push("a0", "a")
+    a = s.admit()
+    s.release(a[2])
+    s.push("b0", "b")
+    s.push("a1", "a")                                   # 'a' has queued work: its idle worker stays
+    g = s.admit()
+    assert g[0] == "a1" and g[2] == a[2] and g[4] == []
+    assert s.admit()[0] is None                         # b0 waits for the budget
