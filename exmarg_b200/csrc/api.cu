@@ -325,18 +325,34 @@ static void ctx_free(exm_ctx *ctx)
 }
 
 static std::mutex g_attr_mu;
-static std::vector<std::pair<int, const void *>> g_attr_done;   // (device, kernel) raised to the opt-in limit
+struct AttrDone {
+    int dev;
+    const void *func;
+    size_t max_dyn;   // the dynamic shared memory the function may take on this device
+};
+static std::vector<AttrDone> g_attr_done;
 
 void exm_allow_smem(exm_ctx *ctx, const void *func, size_t smem)
 {
-    if (smem > ctx->smem_optin)
-        EXM_THROW(EXM_ERR_ARG, "a kernel needs " + std::to_string(smem) + " B of shared memory, above the device's " +
-                                   std::to_string(ctx->smem_optin) + " B");
     std::lock_guard<std::mutex> lock(g_attr_mu);
-    const std::pair<int, const void *> key(ctx->dev, func);
-    if (std::find(g_attr_done.begin(), g_attr_done.end(), key) != g_attr_done.end()) return;
-    EXM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ctx->smem_optin));
-    g_attr_done.push_back(key);
+    size_t max_dyn = 0;
+    bool found = false;
+    for (const AttrDone &d : g_attr_done)
+        if (d.dev == ctx->dev && d.func == func) {
+            max_dyn = d.max_dyn;
+            found = true;
+        }
+    if (!found) {
+        cudaFuncAttributes fa;
+        EXM_CUDA(cudaFuncGetAttributes(&fa, func));
+        // the opt-in limit covers static and dynamic shared memory together
+        max_dyn = ctx->smem_optin > fa.sharedSizeBytes ? ctx->smem_optin - fa.sharedSizeBytes : 0;
+        EXM_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_dyn));
+        g_attr_done.push_back({ctx->dev, func, max_dyn});
+    }
+    if (smem > max_dyn)
+        EXM_THROW(EXM_ERR_ARG, "a kernel needs " + std::to_string(smem) + " B of dynamic shared memory, above the " +
+                                   std::to_string(max_dyn) + " B it may take on this device");
 }
 
 static std::mutex g_destroy_mu;   // orders a parent's deferred free against its children's destroys
@@ -800,7 +816,12 @@ static void run_segment_graph(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
     if (!ctx->graph_exec || memcmp(key, ctx->graph_key, sizeof(key)) != 0) {
         if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
         ctx->graph_exec = nullptr;
-        exm_fft_plan(ctx, 2 * ctx->nm);   // plans and work areas exist before the capture
+        // this segment runs uncaptured: plans, work areas, kernel modules and their attributes
+        // are all in place before the capture, which then records the same launches for the
+        // following segments
+        copy_input(ctx, sl);
+        run_segment(ctx, sl, rs);
+        EXM_CUDA(cudaStreamSynchronize(ctx->stream));
         const long long gen0 = ctx->alloc_gen;
         const bool tim = ctx->tim_on;
         const double taps0 = ctx->node_taps, tlw0 = ctx->tlw, seg0 = ctx->segments;
@@ -836,6 +857,7 @@ static void run_segment_graph(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
         ctx->launches = l0;
         ctx->gather_launches = g0;
         memcpy(ctx->graph_key, key, sizeof(key));
+        return;
     }
     const int h = exm_tim_begin(ctx, 0);
     EXM_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));

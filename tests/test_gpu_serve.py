@@ -31,7 +31,7 @@ def test_graph_replay_matches_plain(name):
     ctx = bank.ctx
     ctx.set_graph(True)
     try:
-        first = _pe(fx, bank)        # captures on segment 0, replays on segment 1
+        first = _pe(fx, bank)        # segment 0 runs and is captured, segment 1 replays
         again = _pe(fx, bank)        # replays both
     finally:
         ctx.set_graph(False)
