@@ -219,6 +219,71 @@ def run_reference(args):
 
 # ----------------------------------------------------------------------------- B200 arm
 
+PREC_SNRS = (5.0, 15.0, 30.0, 50.0)
+
+
+def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, local):
+    """the full workload on tables kept in HBM as float16 (per-node power-of-two scale) and as bfloat16:
+    segments/s, and the ln B error against the float64 oracle on the float32 tables, sampled over
+    args.prec_templates templates of one segment at each SNR in PREC_SNRS (float32 tables alongside)"""
+    import exmarg_b200 as eb
+    from exmarg_b200 import _lib, synth
+    from oracle import restate
+    n_t = min(args.prec_templates, rows.shape[0])
+    idx = np.sort(np.random.default_rng(9).choice(rows.shape[0], n_t, replace=False))
+    cell = restate.cell_weights(rows[idx, 0], rows[idx, 1], rows[idx, 2])
+    segs = [synth.make_segments(1, 90000 + 17 * i, T=T_SEG, fmax=FMAX, snr=snr, mc=25.0, q=0.8, chi=0.1)
+            for i, snr in enumerate(PREC_SNRS)]
+    oracle, oracle_ref = [], []      # float64 throughout; the reference's precision (complex64 filter)
+    for sg in segs:
+        for prec, dst in (("fp64", oracle), ("ref", oracle_ref)):
+            o = restate.pe_intrinsic(restate.read_segments(sg), bank.W[idx], bank.u[idx], rows[idx, 0], rows[idx, 1],
+                                     rows[idx, 2], bank.lo, bank.n_time, store_h, n_loud=N_LOUD, n_random=N_RANDOM,
+                                     seed=0, precision=prec, bank_rows=idx, n_bank=rows.shape[0])
+            dst.append(restate.log_mean(o["ln_lambda"][0], cell))
+    M, P, Q, S = spec.factors(s_nodes)
+    out = {"snr": list(PREC_SNRS), "templates_sampled": n_t,
+           "error": "|ln B - ln B_fp64| over the sampled templates; float64 oracle on the float32 tables"}
+    for dt in ("f32", "f16", "bf16"):
+        ctx, b, st = bank.ctx, bank, store
+        if dt != "f32":
+            ctx = _lib.Context(local)
+            b = bank.clone_for(ctx)
+            st = synth.MemoryStore(spec, s_nodes, TABLE_SEED, tables=[None] * len(s_nodes), table_dtype=dt)
+            st.generator = (M, P, Q, S, TABLE_SEED)
+            eb.prepare(b, st, "volume", 0.1267)
+            ctx.set_gather_cfg(gather_cfg)
+        d = {}
+        try:
+            if dt != "f32":
+                seg = make_inputs(args.warmup + args.prec_steps, 0, args.templates, args.nodes, args.lags)[2]
+                for i in range(args.warmup):
+                    eb.pe_intrinsic(seg, b, st, rows=[i])
+                ctx.timing(True)
+                for i in range(args.warmup, args.warmup + args.prec_steps):
+                    eb.pe_intrinsic(seg, b, st, rows=[i])
+                tm = ctx.timing(False)
+                d["segments_per_s"] = args.prec_steps / (tm["total_ms"] / 1000.0)
+                d["gather_ms"] = tm["gather_ms"] / args.prec_steps
+                d["context_hbm_gb"] = ctx.bytes / 1e9   # tables + bank + workspace
+            errs, errs_ref = [], []
+            for sg, lb, lr in zip(segs, oracle, oracle_ref):
+                r = eb.pe_intrinsic(sg, b, st, rows=[0])
+                v = restate.log_mean(r["ln_lambda"][0][idx], cell)
+                errs.append(abs(v - lb))
+                errs_ref.append(abs(v - lr))
+            d["max_abs_dlnB"] = float(max(errs))
+            d["abs_dlnB_per_snr"] = [float(x) for x in errs]
+            if dt == "f32":   # parity with the reference's own precision at every SNR
+                d["abs_dlnB_vs_reference_per_snr"] = [float(x) for x in errs_ref]
+                d["reference_vs_fp64_per_snr"] = [float(abs(a - c)) for a, c in zip(oracle_ref, oracle)]
+        finally:
+            if dt != "f32":
+                ctx.close()
+        out[dt] = d
+    return out
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """the same segments served by exmarg_b200.serve.Server: child contexts sharing the resident
     tables, two banks (all 2048 templates and the first 1024), graph replay on the workers.
@@ -364,6 +429,9 @@ def run_b200(args):
                                           "times), float64 C gather, %.1f s" % (n_t, N_TEMPLATES, t_cpu)}
         line["parity"] = {"templates": n_t, "max_abs_dlnlambda": float(np.abs(lnl_gpu - lnl_cpu).max()),
                           "sample_dlnB": float(abs(restate.log_mean(lnl_gpu, cell) - restate.log_mean(lnl_cpu, cell)))}
+        if args.prec_templates > 0:
+            cfg = ctx.gather_cfg if ctx.gather_cfg is not None else 0
+            line["precision"] = precision_legs(args, spec, s_nodes, rows, bank, store, store_h, cfg, local)
         del store_h
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -386,6 +454,9 @@ def main():
     ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
     ap.add_argument("--lags", type=int, default=87, help="table lags (reduced profiling cases; odd)")
     ap.add_argument("--gather-cfg", type=int, default=-1, help="force a gather launch shape (no autotuning)")
+    ap.add_argument("--prec-templates", type=int, default=64,
+                    help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
+    ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
     ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
     args = ap.parse_args()

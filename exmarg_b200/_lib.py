@@ -123,6 +123,7 @@ class Context:
         self.bank_token = None
         self.prep_token = None
         self.nm = self.nfreq = self.n_time = None
+        self.gather_cfg = None          # the launch shape chosen by autotune or set_gather_cfg (None: default)
 
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
@@ -264,10 +265,12 @@ class Context:
         best = ctypes.c_int()
         ms = np.zeros(16, np.float64)
         self._check(self.lib.exm_autotune(self.h, int(n_loud), int(n_random), int(reps), ctypes.byref(best), _p(ms)))
+        self.gather_cfg = best.value
         return best.value, ms
 
     def set_gather_cfg(self, cfg):
         self._check(self.lib.exm_set_gather_cfg(self.h, int(cfg)))
+        self.gather_cfg = int(cfg)
 
     def node_values(self, n_nodes):
         out = np.empty((n_nodes + 1, self.nm), np.float64)

@@ -275,6 +275,8 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         ctx->ahi = parent->ahi;
         ctx->node_set = parent->node_set;
         ctx->T.p = parent->T.p;            // borrowed: not counted, not freed
+        ctx->tscale = parent->tscale;
+        ctx->d_tscale.p = parent->d_tscale.p;
         ctx->tstride = parent->tstride;
         ctx->d_tau.p = parent->d_tau.p;
         ctx->tmap = parent->tmap;
@@ -311,13 +313,14 @@ static void ctx_free(exm_ctx *ctx)
     if (ctx->store_borrowed) {   // the parent owns the tables
         ctx->T = dbuf();
         ctx->d_tau = dbuf();
+        ctx->d_tscale = dbuf();
     }
     free_slot(ctx, ctx->slot);
     for (auto &e : ctx->ev_pool) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
-    dbuf *all[] = {&ctx->T, &ctx->d_tau, &ctx->d_W, &ctx->d_bhat_off, &ctx->d_bnode, &ctx->d_cb, &ctx->d_lnW,
+    dbuf *all[] = {&ctx->T, &ctx->d_tau, &ctx->d_tscale, &ctx->d_W, &ctx->d_bhat_off, &ctx->d_bnode, &ctx->d_cb, &ctx->d_lnW,
                    &ctx->d_cell, &ctx->d_mlo, &ctx->d_mhi, &ctx->d_order, &ctx->d_cki, &ctx->d_ckd, &ctx->fftwork, &ctx->d_stats};
     for (dbuf *b : all) exm_free(ctx, *b);
     cudaStreamDestroy(ctx->stream);
@@ -392,7 +395,8 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
     REQUIRE(ntau >= 1 && tau_idx, EXM_ERR_ARG, "need at least one lag");
     REQUIRE(nphif == EXM_NPHI / 2 + 1, EXM_ERR_ARG, "tables must hold NPHI/2 + 1 = 49 phase planes");
     REQUIRE(nb >= 2 && nb <= 4096 && nd >= 2 && nd <= 256, EXM_ERR_ARG, "need 2 <= nb <= 4096 and 2 <= nd <= 256");
-    REQUIRE(dtype == EXM_DTYPE_F32, EXM_ERR_ARG, "this build stores float32 tables");
+    REQUIRE(dtype == EXM_DTYPE_F32 || dtype == EXM_DTYPE_F16 || dtype == EXM_DTYPE_BF16, EXM_ERR_ARG,
+            "dtype must be EXM_DTYPE_F32, EXM_DTYPE_F16 or EXM_DTYPE_BF16");
     REQUIRE(dbeta > 0 && ddelta > 0, EXM_ERR_ARG, "grid steps must be positive");
     ctx->store_ok = ctx->prep_ok = false;
     ctx->tmap_ok = false;
@@ -401,7 +405,8 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
     ctx->nphif = nphif;
     ctx->nb = nb;
     ctx->nd = nd;
-    ctx->ndp = (nd + 3) & ~3;
+    const int al = (int)(16 / exm_dtype_bytes(dtype));   // elements per 16 bytes
+    ctx->ndp = (nd + al - 1) / al * al;
     ctx->dtype = dtype;
     ctx->beta0 = beta0;
     ctx->dbeta = dbeta;
@@ -414,8 +419,12 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
     ctx->node_set.assign(n_nodes, 0);
     ctx->tstride = (size_t)ntau * nphif * nb * ctx->ndp;
     exm_free(ctx, ctx->T);
-    exm_alloc(ctx, ctx->T, ctx->tstride * n_nodes * sizeof(float));
+    exm_alloc(ctx, ctx->T, ctx->tstride * n_nodes * exm_dtype_bytes(dtype));
     EXM_CUDA(cudaMemsetAsync(ctx->T.p, 0, ctx->T.bytes, ctx->stream));
+    ctx->tscale.assign(n_nodes, 1.f);
+    exm_ensure(ctx, ctx->d_tscale, sizeof(float) * EXM_MAX_NODES);
+    EXM_CUDA(cudaMemcpyAsync(ctx->d_tscale.p, ctx->tscale.data(), sizeof(float) * n_nodes, cudaMemcpyHostToDevice,
+                             ctx->stream));
     std::vector<int> t32(ntau);
     for (int r = 0; r < ntau; ++r) t32[r] = (int)tau_idx[r];
     exm_ensure(ctx, ctx->d_tau, sizeof(int) * ntau);
@@ -449,10 +458,18 @@ extern "C" int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(T, EXM_ERR_ARG, "null table");
     set_node_meta(ctx, k, s, alpha_lo, alpha_hi);
-    float *dst = (float *)ctx->T.p + (size_t)k * ctx->tstride;
     const size_t rows = (size_t)ctx->ntau * ctx->nphif * ctx->nb;
-    EXM_CUDA(cudaMemcpy2DAsync(dst, ctx->ndp * sizeof(float), T, ctx->nd * sizeof(float), ctx->nd * sizeof(float),
-                               rows, cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->dtype == EXM_DTYPE_F32) {
+        float *dst = (float *)ctx->T.p + (size_t)k * ctx->tstride;
+        EXM_CUDA(cudaMemcpy2DAsync(dst, ctx->ndp * sizeof(float), T, ctx->nd * sizeof(float), ctx->nd * sizeof(float),
+                                   rows, cudaMemcpyHostToDevice, ctx->stream));
+    } else {   // the float32 node through a scratch copy, quantized on the device
+        dbuf f;
+        exm_alloc(ctx, f, sizeof(float) * rows * ctx->nd);
+        EXM_CUDA(cudaMemcpyAsync(f.p, T, sizeof(float) * rows * ctx->nd, cudaMemcpyHostToDevice, ctx->stream));
+        exm_store_quantize(ctx, k, (const float *)f.p, ctx->nd);
+        exm_free(ctx, f);
+    }
     EXM_CUDA(cudaStreamSynchronize(ctx->stream));
     API_END(ctx)
 }
@@ -475,11 +492,20 @@ extern "C" int exm_store_get_node(exm_ctx *ctx, int k, float *T_out)
     API_BEGIN(ctx)
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(ctx->T.p && k >= 0 && k < ctx->nn && T_out, EXM_ERR_ARG, "bad node or output");
-    const float *src = (const float *)ctx->T.p + (size_t)k * ctx->tstride;
     const size_t rows = (size_t)ctx->ntau * ctx->nphif * ctx->nb;
-    EXM_CUDA(cudaMemcpy2DAsync(T_out, ctx->nd * sizeof(float), src, ctx->ndp * sizeof(float), ctx->nd * sizeof(float),
-                               rows, cudaMemcpyDeviceToHost, ctx->stream));
-    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->dtype == EXM_DTYPE_F32) {
+        const float *src = (const float *)ctx->T.p + (size_t)k * ctx->tstride;
+        EXM_CUDA(cudaMemcpy2DAsync(T_out, ctx->nd * sizeof(float), src, ctx->ndp * sizeof(float),
+                                   ctx->nd * sizeof(float), rows, cudaMemcpyDeviceToHost, ctx->stream));
+        EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    } else {   // the values scale * element, as float32
+        dbuf f;
+        exm_alloc(ctx, f, sizeof(float) * rows * ctx->nd);
+        exm_store_dequantize(ctx, k, (float *)f.p, ctx->nd);
+        EXM_CUDA(cudaMemcpyAsync(T_out, f.p, sizeof(float) * rows * ctx->nd, cudaMemcpyDeviceToHost, ctx->stream));
+        EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+        exm_free(ctx, f);
+    }
     API_END(ctx)
 }
 

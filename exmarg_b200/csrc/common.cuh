@@ -92,8 +92,10 @@ struct exm_ctx {
     std::vector<int64_t> tau;
     std::vector<double> s, alo, ahi;
     std::vector<char> node_set;
-    dbuf T;             // [nn][ntau][nphif][nb][ndp]
+    dbuf T;             // [nn][ntau][nphif][nb][ndp] of float32, float16 or bfloat16 (dtype)
     size_t tstride = 0; // elements per node
+    std::vector<float> tscale;   // per node: value = tscale[k] * stored element (1 for float32, bfloat16)
+    dbuf d_tscale;               // float [nn]
     dbuf d_tau;         // int32 [ntau]
     CUtensorMap tmap;   // 5-D map over T for the plane windows
     bool tmap_ok = false;

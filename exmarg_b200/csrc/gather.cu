@@ -16,11 +16,15 @@
 //
 // k_gather_simple (the gather_cpu / gather_gpu contract, any table per slot): one
 // block per (row, lag), the reference's arithmetic in float64.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
-#define SLOT_FLOATS (EXM_WB * EXM_WD)
-#define SLOT_BYTES (SLOT_FLOATS * 4)
+// one staged (node, lag, plane) window of element type TE: EXM_WB rows x TabElem<TE>::wd columns
+template <typename TE> __host__ __device__ constexpr int slot_elems() { return EXM_WB * TabElem<TE>::wd; }
+template <typename TE> __host__ __device__ constexpr unsigned slot_bytes() { return (unsigned)(slot_elems<TE>() * sizeof(TE)); }
+static_assert(slot_bytes<float>() % 128 == 0 && slot_bytes<__half>() % 128 == 0, "slots keep 128-byte alignment");
 #define EXM_WAIT_CYCLES (2000000000LL)   // about one second at 1.9 GHz
 
 struct PlaneArgs {
@@ -28,7 +32,7 @@ struct PlaneArgs {
     const int32_t *tside;
     const int *off;
     const float2 *H, *L;
-    const float *T;
+    const void *T;               // node tables, element type of the kernel's TE
     const int *mlo, *mhi, *bnode, *win, *tau;
     const double *boff, *cb, *ckd;
     double *part;
@@ -40,6 +44,7 @@ struct PlaneArgs {
     double rph, rdb, rdd, offd;
     int cki[EXM_MAX_NODES];
     float ckf[EXM_MAX_NODES];
+    float tsc[EXM_MAX_NODES];    // per node: value = tsc * stored element
 };
 
 // ------------------------------------------------------------------ TMA + mbarrier
@@ -51,7 +56,7 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
-__device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t *bar, float *dst, int x, int y, int z,
+__device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t *bar, void *dst, int x, int y, int z,
                                                int w, int v, unsigned bytes)
 {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -116,18 +121,28 @@ __device__ __forceinline__ bool seg_reduce(int id, float &B, float &E, float &S)
 }
 
 // bilinear in (beta, Delta) on planes p and p+1 of the staged windows, linear in phase;
-// value = t00 + eps with t00 the stored value at (p, b0, d0)
-__device__ __forceinline__ void interp_window(const float *s0, const float *s1, int o, float fbf, float fd, float w,
+// value = t00 + eps with t00 the stored value at (p, b0, d0).  16-bit elements are
+// interpolated as stored (float32 arithmetic) and the result scaled by the node's power-of-two
+// scale, which is exact.
+template <typename TE>
+__device__ __forceinline__ void interp_window(const TE *s0, const TE *s1, int o, float fbf, float fd, float w, float sc,
                                               float &B, float &E)
 {
-    const float t00 = s0[o], t01 = s0[o + 1], t10 = s0[o + EXM_WD], t11 = s0[o + EXM_WD + 1];
-    const float u00 = s1[o], u01 = s1[o + 1], u10 = s1[o + EXM_WD], u11 = s1[o + EXM_WD + 1];
+    constexpr int WD = TabElem<TE>::wd;
+    const float t00 = TabElem<TE>::cvt(s0[o]), t01 = TabElem<TE>::cvt(s0[o + 1]);
+    const float t10 = TabElem<TE>::cvt(s0[o + WD]), t11 = TabElem<TE>::cvt(s0[o + WD + 1]);
+    const float u00 = TabElem<TE>::cvt(s1[o]), u01 = TabElem<TE>::cvt(s1[o + 1]);
+    const float u10 = TabElem<TE>::cvt(s1[o + WD]), u11 = TabElem<TE>::cvt(s1[o + WD + 1]);
     const float a0 = t01 - t00, c0 = t10 - t00, e0 = (t11 - t10) - a0;
     const float eps0 = fmaf(fd, a0, fbf * fmaf(fd, e0, c0));
     const float a1 = u01 - u00, c1 = u10 - u00, e1 = (u11 - u10) - a1;
     const float eps1 = fmaf(fd, a1, fbf * fmaf(fd, e1, c1));
     B = t00;
     E = fmaf(w, (u00 - t00) + (eps1 - eps0), eps0);
+    if (!std::is_same<TE, float>::value) {
+        B *= sc;
+        E *= sc;
+    }
 }
 
 __device__ __forceinline__ void split_double(double v, float &B, float &E)
@@ -143,7 +158,8 @@ __device__ __forceinline__ void split_double(double v, float &B, float &E)
 struct RunCtx {
     const uint4 *descr;
     const int32_t *tsr;
-    const float *s0, *s1;
+    const void *s0, *s1;        // the staged windows of planes p and p + 1 (element type TE)
+    float sc;                   // the node's scale (16-bit tables)
     float *aB, *aE, *aS;        // accumulators of the run's templates, index t - lo
     const int *bci;             // boundary runs: per-template integer offset (index t - lo)
     const float *bcf;           //                and fraction
@@ -154,40 +170,6 @@ struct RunCtx {
     int tF, tL;                 // the templates at the two ends of this warp's taps (may be shared with
     float *eF, *eL;             // neighbouring warps): their partials go to this warp's edge slots
 };
-
-template <bool BND>
-__device__ __forceinline__ void tap_value(const PlaneArgs &a, const RunCtx &c, uint4 q, int j, int tr, float &vB,
-                                          float &vE, unsigned &n_slow)
-{
-    const int il = (int)(q.w >> 19);
-    const float fb = __uint_as_float(q.x), fd = __uint_as_float(q.y);
-    const float w = __uint_as_float(q.z & 0x7FFFFFFFu);
-    const float lwv = (q.z >> 31) ? c.lw : 0.f;
-    const int d0 = (int)((q.w >> 11) & 0xFFu);
-    const int ibh = ((int)(q.w << 21)) >> 21;
-    const float sfr = fb + (BND ? c.bcf[tr] : c.ckf);
-    const int cy = sfr >= 1.f;
-    const float fbf = cy ? sfr - 1.f : sfr;
-    const int b0 = ibh + (BND ? c.bci[tr] : c.cki) + cy;
-    const int rb = b0 - c.R0, rd = d0 - c.C0;
-    const bool fast = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
-                      b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf > 0.999999f);
-    if (fast) {
-        interp_window(c.s0, c.s1, rb * EXM_WD + rd, fbf, fd, w, vB, vE);
-    } else {
-        ++n_slow;
-        const int t = c.tsr[j];
-        int i1 = t + c.tau0;
-        if (i1 >= c.nt) i1 -= c.nt;
-        const int gi = il + c.m_base;
-        const double offb = (BND ? a.cb[gi] : c.offb_node) + a.boff[gi];
-        const double v = exm_tap_fp64<float>(a.L[(long long)il * c.nt + t], a.H[(long long)il * c.nt + i1], offb, c.r,
-                                             a.T + (long long)c.k * a.tstride, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
-                                             a.rdd, a.offd);
-        split_double(v, vB, vE);
-    }
-    vE += lwv;
-}
 
 __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, float E, float S)
 {
@@ -239,7 +221,7 @@ __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, flo
 
 // GRP taps: decode, window interpolation for all of them (no branch between the shared loads),
 // the exact float64 value for the rare taps outside the window, then the merges
-template <bool BND, int GRP>
+template <bool BND, int GRP, typename TE>
 __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, const uint4 *q, int j, int end, int &cT,
                                           float &cB, float &cE, float &cS, int &fT, float &fB, float &fE, float &fS,
                                           unsigned &n_slow)
@@ -268,12 +250,14 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         fbf[u] = cy ? sfr - 1.f : sfr;
         const int b0 = ibh + (BND ? c.bci[ts] : c.cki) + cy;
         const int rb = b0 - c.R0, rd = d0 - c.C0;
-        fast[u] = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(EXM_WD - 2) &&
+        constexpr int WD = TabElem<TE>::wd;
+        fast[u] = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(WD - 2) &&
                   b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf[u] > 0.999999f);
-        o[u] = min(max(rb, 0), EXM_WB - 2) * EXM_WD + min(max(rd, 0), EXM_WD - 2);
+        o[u] = min(max(rb, 0), EXM_WB - 2) * WD + min(max(rd, 0), WD - 2);
     }
 #pragma unroll
-    for (int u = 0; u < GRP; ++u) interp_window(c.s0, c.s1, o[u], fbf[u], fd[u], w[u], vB[u], vE[u]);
+    for (int u = 0; u < GRP; ++u)
+        interp_window<TE>((const TE *)c.s0, (const TE *)c.s1, o[u], fbf[u], fd[u], w[u], c.sc, vB[u], vE[u]);
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
         if (t[u] >= 0 && !fast[u]) {
@@ -284,9 +268,9 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
             if (i1 >= c.nt) i1 -= c.nt;
             const int gi = il + c.m_base;
             const double offb = (BND ? a.cb[gi] : c.offb_node) + a.boff[gi];
-            const double v = exm_tap_fp64<float>(a.L[(long long)il * c.nt + tm], a.H[(long long)il * c.nt + i1], offb,
-                                                 c.r, a.T + (long long)c.k * a.tstride, a.nphif, a.nb, a.nd, a.ndp,
-                                                 a.rph, a.rdb, a.rdd, a.offd);
+            const double v = exm_tap_fp64<TE>(a.L[(long long)il * c.nt + tm], a.H[(long long)il * c.nt + i1], offb,
+                                              c.r, (const TE *)a.T + (long long)c.k * a.tstride, c.sc, a.nphif, a.nb,
+                                              a.nd, a.ndp, a.rph, a.rdb, a.rdd, a.offd);
             split_double(v, vB[u], vE[u]);
         }
     }
@@ -294,7 +278,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
     for (int u = 0; u < GRP; ++u) lane_merge(c, t[u], vB[u], vE[u] + lwv[u], cT, cB, cE, cS, fT, fB, fE, fS);
 }
 
-template <bool BND, int GRP>
+template <bool BND, int GRP, typename TE>
 __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
 {
     const int lane = threadIdx.x & 31;
@@ -318,7 +302,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
                 for (int u = 0; u < GRP; ++u)
                     qa[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
             }
-            tap_group<BND, GRP>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
+            tap_group<BND, GRP, TE>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
         }
         // the first closed template of lane l + 1 continues lane l's last one, or is lane l + 1's alone
         const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
@@ -384,7 +368,7 @@ __device__ __forceinline__ void fold_edges(float *edge, int nw, float *aB, float
 }
 
 // this warp's equal share [w0, w1) of the run [beg, end), with its edge templates and slots
-template <bool BND, int GRP, int NW>
+template <bool BND, int GRP, int NW, typename TE>
 __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, float *edge,
                                            unsigned &n_slow)
 {
@@ -412,16 +396,18 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     c.tL = tL;
     c.eF = e;
     c.eL = e + 4;
-    if (w0 < w1) process_run<BND, GRP>(a, c, w0, w1, n_slow);
+    if (w0 < w1) process_run<BND, GRP, TE>(a, c, w0, w1, n_slow);
 }
 
-template <int NW, int GRP>
+template <int NW, int GRP, typename TE>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
 {
+    constexpr int SLOT = slot_elems<TE>();
+    constexpr unsigned SLOT_B = slot_bytes<TE>();
     extern __shared__ __align__(1024) unsigned char smem[];
-    float *win = (float *)smem;
-    uint64_t *mbar = (uint64_t *)(smem + 3 * SLOT_BYTES);
-    float *aB = (float *)(smem + 3 * SLOT_BYTES + 64);
+    TE *win = (TE *)smem;
+    uint64_t *mbar = (uint64_t *)(smem + 3 * SLOT_B);
+    float *aB = (float *)(smem + 3 * SLOT_B + 64);
     const int tch = a.tch;
     float *aE = aB + tch, *aS = aE + tch;
     float *bB = aS + tch, *bE = bB + tch, *bS = bE + tch;
@@ -471,8 +457,8 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     __syncthreads();
     const int blo = bl_sh[0], bhi = bl_sh[1];
     if (tid == 0) {
-        tma_load_plane(&tmap, &mbar[0], win, C0, R0, 0, r, k, SLOT_BYTES);
-        tma_load_plane(&tmap, &mbar[1], win + SLOT_FLOATS, C0, R0, 1, r, k, SLOT_BYTES);
+        tma_load_plane(&tmap, &mbar[0], win, C0, R0, 0, r, k, SLOT_B);
+        tma_load_plane(&tmap, &mbar[1], win + SLOT, C0, R0, 1, r, k, SLOT_B);
     }
     int issued = 2;
 
@@ -491,6 +477,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     rc.C0 = C0;
     rc.cki = a.cki[k];
     rc.ckf = a.ckf[k];
+    rc.sc = a.tsc[k];
     rc.k = k;
     rc.r = r;
     rc.tau0 = ((a.tau[r] % nt) + nt) % nt;
@@ -512,25 +499,25 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         }
         if (tid == 0 && ok && p + 2 < a.nphif) {
             const int q = p + 2;
-            tma_load_plane(&tmap, &mbar[q % 3], win + (q % 3) * SLOT_FLOATS, C0, R0, q, r, k, SLOT_BYTES);
+            tma_load_plane(&tmap, &mbar[q % 3], win + (q % 3) * SLOT, C0, R0, q, r, k, SLOT_B);
             ++issued;
         }
         ok = ok && mbar_wait(&mbar[(p + 1) % 3], ((p + 1) / 3) & 1, a.err);
         if (!ok) continue;
-        rc.s0 = win + (p % 3) * SLOT_FLOATS;
-        rc.s1 = win + ((p + 1) % 3) * SLOT_FLOATS;
+        rc.s0 = win + (p % 3) * SLOT;
+        rc.s1 = win + ((p + 1) % 3) * SLOT;
         const int *offp = offr + p * (a.nmc + 1) + base_i;
         rc.aB = aB;
         rc.aE = aE;
         rc.aS = aS;
-        warp_share<false, GRP, NW>(a, rc, offp[0], offp[n], edge[0], n_slow);
+        warp_share<false, GRP, NW, TE>(a, rc, offp[0], offp[n], edge[0], n_slow);
         if (blo < bhi) {
             rc.aB = bB;
             rc.aE = bE;
             rc.aS = bS;
             const int bb = offp[blo], be = offp[bhi];
             n_bnd += (lane == 0 && (tid >> 5) == 0) ? (unsigned)(be - bb) : 0u;
-            warp_share<true, GRP, NW>(a, rc, bb, be, edge[1], n_slow);
+            warp_share<true, GRP, NW, TE>(a, rc, bb, be, edge[1], n_slow);
         }
     }
     __syncthreads();
@@ -570,29 +557,41 @@ struct GatherCfg {
 static const GatherCfg kGatherCfgs[] = {{16, 4}, {16, 2}, {24, 2}, {32, 2}, {32, 1}};
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
-template <int NW, int GRP>
+template <int NW, int GRP, typename TE>
 static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
 {
-    exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP>, smem);
-    k_gather_planes<NW, GRP><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+    exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP, TE>, smem);
+    k_gather_planes<NW, GRP, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+}
+
+template <typename TE>
+static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
+{
+    switch (cfg) {
+    case 0: launch_planes<16, 4, TE>(ctx, a, grid, smem); break;
+    case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    case 3: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
+    default: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
+    }
 }
 
 static void launch_cfg(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
-    switch (cfg) {
-    case 0: launch_planes<16, 4>(ctx, a, grid, smem); break;
-    case 1: launch_planes<16, 2>(ctx, a, grid, smem); break;
-    case 2: launch_planes<24, 2>(ctx, a, grid, smem); break;
-    case 3: launch_planes<32, 2>(ctx, a, grid, smem); break;
-    default: launch_planes<32, 1>(ctx, a, grid, smem); break;
-    }
+    if (ctx->dtype == EXM_DTYPE_F16)
+        launch_cfg_t<__half>(ctx, cfg, a, grid, smem);
+    else if (ctx->dtype == EXM_DTYPE_BF16)
+        launch_cfg_t<__nv_bfloat16>(ctx, cfg, a, grid, smem);
+    else
+        launch_cfg_t<float>(ctx, cfg, a, grid, smem);
 }
 
 int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 
-static size_t planes_smem(int tch)
+static size_t planes_smem(int tch, int dtype)
 {
-    return (size_t)3 * SLOT_BYTES + 64 + (size_t)tch * 8 * 4;
+    const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
+    return 3 * slot + 64 + (size_t)tch * 8 * 4;
 }
 
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc)
@@ -605,7 +604,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.off = (const int *)sl.cnt.p;
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ci.nmc * ctx->nt;
-    a.T = (const float *)ctx->T.p;
+    a.T = ctx->T.p;
     a.mlo = (const int *)ctx->d_mlo.p;
     a.mhi = (const int *)ctx->d_mhi.p;
     a.bnode = (const int *)ctx->d_bnode.p;
@@ -639,6 +638,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
         const double f = std::floor(ctx->ck[k]);
         a.cki[k] = (int)f;
         a.ckf[k] = (float)(ctx->ck[k] - f);
+        a.tsc[k] = ctx->tscale[k];
     }
     // templates per block: about one wave of blocks per lag, so that the descriptors of the lag
     // in flight stay in L2; at most EXM_TCH (shared-memory accumulators)
@@ -655,7 +655,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     tch = std::min(((tch + 15) / 16) * 16, EXM_TCH);
     a.tch = tch;
     a.nch = (maxn + tch - 1) / tch;
-    const size_t smem = planes_smem(tch);
+    const size_t smem = planes_smem(tch, ctx->dtype);
     dim3 grid(rc * ctx->nn * a.nch);
     const int cfg = (ctx->gather_cfg >= 0 && ctx->gather_cfg < kNumGatherCfgs) ? ctx->gather_cfg : 0;
     launch_cfg(ctx, cfg, a, grid, smem);
@@ -678,7 +678,8 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
 struct SimpleArgs {
     const float2 *H, *L;
     const int32_t *sel;
-    const float *T;
+    const void *T;              // node tables (element type TE of the kernel)
+    const float *tsc;           // per node scale
     const int *rows, *tab, *tau;
     const double *lna;
     double *om, *os;
@@ -688,6 +689,7 @@ struct SimpleArgs {
     double beta0, dbeta, rph, rdb, rdd, offd;
 };
 
+template <typename TE>
 __global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
 {
     __shared__ double shm[8], shs[8];
@@ -698,7 +700,9 @@ __global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
     const float2 *H = a.H + (long long)row * nt, *L = a.L + (long long)row * nt;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int n = 0; n < a.ns; ++n) {
-        const float *Tn = a.T + (long long)a.tab[j * a.ns + n] * a.tstride;
+        const int tb = a.tab[j * a.ns + n];
+        const TE *Tn = (const TE *)a.T + (long long)tb * a.tstride;
+        const float sc = a.tsc[tb];
         const double offb = (a.lna[j * a.ns + n] - a.beta0) / a.dbeta;
         double m = -1e300, s = 0.0;
         for (int kk = threadIdx.x; kk < a.nwalk; kk += blockDim.x) {
@@ -710,8 +714,8 @@ __global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
             }
             int i1 = t + tau0;
             if (i1 >= nt) i1 -= nt;
-            double acc = exm_tap_fp64<float>(L[t], H[i1], offb, r, Tn, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
-                                             a.rdd, a.offd);
+            double acc = exm_tap_fp64<TE>(L[t], H[i1], offb, r, Tn, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
+                                          a.rdd, a.offd);
             if (a.use_sel) acc += flag ? (double)a.lw : 0.0;
             if (acc > m) {
                 s = s * exp(m - acc) + 1.0;
@@ -775,7 +779,8 @@ void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const i
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ctx->nm * ctx->nt;
     a.sel = (const int32_t *)sl.sel.p;
-    a.T = (const float *)ctx->T.p;
+    a.T = ctx->T.p;
+    a.tsc = (const float *)ctx->d_tscale.p;
     a.rows = d_rows;
     a.tab = d_tab;
     a.tau = (const int *)ctx->d_tau.p;
@@ -801,7 +806,12 @@ void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const i
     a.rdd = 1.0 / ctx->ddelta;
     a.offd = -ctx->delta0 / ctx->ddelta;
     dim3 grid(nsel, ctx->ntau);
-    k_gather_simple<<<grid, 256, 0, ctx->stream>>>(a);
+    if (ctx->dtype == EXM_DTYPE_F16)
+        k_gather_simple<__half><<<grid, 256, 0, ctx->stream>>>(a);
+    else if (ctx->dtype == EXM_DTYPE_BF16)
+        k_gather_simple<__nv_bfloat16><<<grid, 256, 0, ctx->stream>>>(a);
+    else
+        k_gather_simple<float><<<grid, 256, 0, ctx->stream>>>(a);
     k_lse_lags<<<(ns * nsel + 255) / 256, 256, 0, ctx->stream>>>(a.om, a.os, ns, ctx->ntau, nsel, ctx->nt, d_out);
     EXM_CUDA(cudaGetLastError());
 }

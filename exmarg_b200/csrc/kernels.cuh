@@ -1,5 +1,8 @@
 // Device helpers shared by the kernels, and the host-side launchers of each stage.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 
@@ -7,7 +10,38 @@
 
 // staging window of one (node, lag, phase plane): rows of beta x columns of Delta
 #define EXM_WB 80
-#define EXM_WD 164   // row pitch = 4 banks mod 32: neighbouring rows start on different banks
+#define EXM_WD 164     // float32 tables: row pitch = 4 banks mod 32, neighbouring rows start on different banks
+#define EXM_WD16 168   // 16-bit tables: a multiple of 8 elements (16-byte TMA rows), pitch 20 banks mod 32
+
+// Table elements as stored: float32, or 16-bit with a per-node scale (value = scale * element;
+// the scale is a power of two for float16 and 1 for bfloat16, so the product is exact).
+template <typename TE> struct TabElem;
+template <> struct TabElem<float> {
+    static constexpr int wd = EXM_WD;
+    static constexpr int calign = 4;   // window column origin: a multiple of 16 bytes
+    static constexpr CUtensorMapDataType tma = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    __device__ static __forceinline__ float ld(const float *p) { return __ldg(p); }
+    __device__ static __forceinline__ float cvt(float v) { return v; }
+};
+template <> struct TabElem<__half> {
+    static constexpr int wd = EXM_WD16;
+    static constexpr int calign = 8;
+    static constexpr CUtensorMapDataType tma = CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    __device__ static __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
+    __device__ static __forceinline__ float cvt(__half v) { return __half2float(v); }
+};
+template <> struct TabElem<__nv_bfloat16> {
+    static constexpr int wd = EXM_WD16;
+    static constexpr int calign = 8;
+    static constexpr CUtensorMapDataType tma = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    __device__ static __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
+    __device__ static __forceinline__ float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
+};
+
+// bytes per stored element, window columns and column alignment of a store dtype (EXM_DTYPE_*)
+inline size_t exm_dtype_bytes(int dtype) { return dtype == EXM_DTYPE_F32 ? 4 : 2; }
+inline int exm_dtype_wd(int dtype) { return dtype == EXM_DTYPE_F32 ? EXM_WD : EXM_WD16; }
+inline int exm_dtype_calign(int dtype) { return dtype == EXM_DTYPE_F32 ? 4 : 8; }
 #define EXM_TCH 2048        // templates per gather block
 #define EXM_MAX_CHUNK 8192  // templates per pass (13-bit template field of a descriptor)
 #define EXM_MAX_NODES 64
@@ -54,18 +88,12 @@ __device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, double boff, co
 }
 
 // the reference's tap value in float64 (exmarg/search/gather.py:50-93) for one
-// node table Tn (padded rows of ndp floats), lag row r; lw added by the caller
-template <typename TT>
-__device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, int r, const TT *__restrict__ Tn,
-                                               int nphif, int nb, int nd, int ndp, double rph, double rdb, double rdd,
-                                               double offd);
-
-__device__ __forceinline__ float exm_ld(const float *p) { return __ldg(p); }
-
-template <>
-__device__ __forceinline__ double exm_tap_fp64<float>(float2 l, float2 h, double offb, int r,
-                                                      const float *__restrict__ Tn, int nphif, int nb, int nd, int ndp,
-                                                      double rph, double rdb, double rdd, double offd)
+// node table Tn (padded rows of ndp elements, value = scale * element), lag row r;
+// lw added by the caller
+template <typename TE>
+__device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, int r, const TE *__restrict__ Tn,
+                                               float scale, int nphif, int nb, int nd, int ndp, double rph, double rdb,
+                                               double rdd, double offd)
 {
     double x3 = (double)(h.y - l.y) * rph;
     if (x3 < 0.0) x3 += EXM_NPHI;
@@ -93,16 +121,19 @@ __device__ __forceinline__ double exm_tap_fp64<float>(float2 l, float2 h, double
         int ci = cc ? c1 : c0;
         if (ci > EXM_NPHI / 2) ci = EXM_NPHI - ci;
         const double fci = cc ? fc : 1.0 - fc;
-        const float *r0 = Tn + (((long long)r * nphif + ci) * nb + b0) * ndp;
-        const float *r1 = Tn + (((long long)r * nphif + ci) * nb + b1) * ndp;
-        const double v = fb0 * (fd0 * (double)exm_ld(r0 + d0) + fdf * (double)exm_ld(r0 + d1)) +
-                         fbf * (fd0 * (double)exm_ld(r1 + d0) + fdf * (double)exm_ld(r1 + d1));
+        const TE *r0 = Tn + (((long long)r * nphif + ci) * nb + b0) * ndp;
+        const TE *r1 = Tn + (((long long)r * nphif + ci) * nb + b1) * ndp;
+        const double v = fb0 * (fd0 * (double)TabElem<TE>::ld(r0 + d0) + fdf * (double)TabElem<TE>::ld(r0 + d1)) +
+                         fbf * (fd0 * (double)TabElem<TE>::ld(r1 + d0) + fdf * (double)TabElem<TE>::ld(r1 + d1));
         acc += fci * v;
     }
-    return acc;
+    return acc * (double)scale;
 }
 
 // ------------------------------------------------------------------ launchers
+
+void exm_store_quantize(exm_ctx *ctx, int k, const float *src, int sp);
+void exm_store_dequantize(exm_ctx *ctx, int k, float *dst, int dp);
 
 void exm_fft_plan(exm_ctx *ctx, int batch);
 void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm);

@@ -57,7 +57,8 @@ struct NoAllocArgs {
     const float *lw;
     const int64_t *ids, *tab;
     const double *lna;
-    const float *T;
+    const void *T;              // node tables (element type TE of the kernel)
+    const float *tsc;           // per node scale
     const int *tau;
     double *om, *os;
     unsigned *err;
@@ -67,6 +68,7 @@ struct NoAllocArgs {
 };
 
 // one block per (row, lag): running (max, sum) over the walked times, float64, per slot
+template <typename TE>
 __global__ void __launch_bounds__(256) k_gather_noalloc(NoAllocArgs a)
 {
     __shared__ double shm[8], shs[8];
@@ -93,8 +95,8 @@ __global__ void __launch_bounds__(256) k_gather_noalloc(NoAllocArgs a)
             if (i1 >= nt) i1 -= nt;
             const float2 l = make_float2(a.lqL[mid * nt + t], a.phL[mid * nt + t]);
             const float2 h = make_float2(a.lqH[mid * nt + i1], a.phH[mid * nt + i1]);
-            double acc = exm_tap_fp64<float>(l, h, offb, r, a.T + tb * a.tstride, a.nphif, a.nb, a.nd, a.ndp, a.rph,
-                                             a.rdb, a.rdd, a.offd);
+            double acc = exm_tap_fp64<TE>(l, h, offb, r, (const TE *)a.T + tb * a.tstride, a.tsc[tb], a.nphif, a.nb,
+                                          a.nd, a.ndp, a.rph, a.rdb, a.rdd, a.offd);
             if (a.sel) acc += (double)a.lw[mid * a.nwalk + k];
             if (acc > m) {
                 s = s * exp(m - acc) + 1.0;
@@ -185,7 +187,8 @@ extern "C" int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float 
         a.ids = mass_ids;
         a.tab = tab_ids;
         a.lna = lna;
-        a.T = (const float *)ctx->T.p;
+        a.T = ctx->T.p;
+        a.tsc = (const float *)ctx->d_tscale.p;
         a.tau = (const int *)ctx->d_tau.p;
         a.om = scratch;
         a.os = scratch + EXM_NOALLOC_MAX_ENTRIES;
@@ -209,7 +212,12 @@ extern "C" int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float 
         a.rdd = 1.0 / ctx->ddelta;
         a.offd = -ctx->delta0 / ctx->ddelta;
         dim3 grid(nsel, ctx->ntau);
-        k_gather_noalloc<<<grid, 256, 0, ctx->stream>>>(a);
+        if (ctx->dtype == EXM_DTYPE_F16)
+            k_gather_noalloc<__half><<<grid, 256, 0, ctx->stream>>>(a);
+        else if (ctx->dtype == EXM_DTYPE_BF16)
+            k_gather_noalloc<__nv_bfloat16><<<grid, 256, 0, ctx->stream>>>(a);
+        else
+            k_gather_noalloc<float><<<grid, 256, 0, ctx->stream>>>(a);
         k_gather_noalloc_lags<<<(ns * nsel + 255) / 256, 256, 0, ctx->stream>>>(a.om, a.os, ns, ctx->ntau, nsel, n_time,
                                                                                out);
         EXM_CUDA(cudaGetLastError());

@@ -242,19 +242,20 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     }
 }
 
-// staging-window origins: column C0 (a multiple of 4) and, per node, the first beta row
+// staging-window origins: column C0 (a multiple of calign elements, 16 bytes) and, per node,
+// the first beta row; wd columns per window
 __global__ void k_windows(const int *hist_b, const int *hist_d, const int *cki, int nn, int nb, int nd, int ndp,
-                          int *win)
+                          int wd, int calign, int *win)
 {
     __shared__ long long best[2];
     if (threadIdx.x == 0) best[0] = best[1] = 0;
     __syncthreads();
-    // columns: d0 in [C0, C0 + WD - 2]
-    const int cmax = max(0, ndp - EXM_WD);
-    for (int c0 = threadIdx.x * 4; c0 <= cmax; c0 += blockDim.x * 4) {
+    // columns: d0 in [C0, C0 + wd - 2]
+    const int cmax = max(0, ndp - wd);
+    for (int c0 = threadIdx.x * calign; c0 <= cmax; c0 += blockDim.x * calign) {
         long long s = 0;
-        for (int d = c0; d <= min(c0 + EXM_WD - 2, nd - 1); ++d) s += hist_d[d];
-        long long key = (s << 12) | (4095 - (c0 >> 2));
+        for (int d = c0; d <= min(c0 + wd - 2, nd - 1); ++d) s += hist_d[d];
+        long long key = (s << 12) | (4095 - c0 / calign);
         atomicMax((unsigned long long *)&best[0], (unsigned long long)key);
     }
     // beta-hat rows: ib in [Rh, Rh + WB - 3]
@@ -266,7 +267,7 @@ __global__ void k_windows(const int *hist_b, const int *hist_d, const int *cki, 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        win[0] = (4095 - (int)(best[0] & 4095)) * 4;
+        win[0] = (4095 - (int)(best[0] & 4095)) * calign;
         const int rh = (4095 - (int)(best[1] & 4095)) + EXM_HB_LO;
         for (int k = 0; k < nn; ++k) {
             int r0 = rh + cki[k];
@@ -311,7 +312,7 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     k_tap_scan<<<rc, 1024, 0, ctx->stream>>>(a.cnt, ci.nmc);
     k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
-                                          (int *)sl.win.p);
+                                          exm_dtype_wd(ctx->dtype), exm_dtype_calign(ctx->dtype), (int *)sl.win.p);
     EXM_CUDA(cudaGetLastError());
     ctx->launches += 4;
 }

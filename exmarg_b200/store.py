@@ -62,11 +62,19 @@ class RedshiftStore:
     tables: list
     n_max: int
     device_tokens: dict = field(default_factory=dict, repr=False)
+    table_dtype: str = "f32"
 
 
-def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False):
+TABLE_DTYPES = {"f32": _lib.DTYPE_F32, "f16": _lib.DTYPE_F16, "bf16": _lib.DTYPE_BF16}
+
+
+def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dtype="f32"):
     """every node of the store in host memory (about 0.75 GB per node at the production shape);
-    pinned is accepted for the reference's signature (the b200 path copies each table to HBM once)"""
+    pinned is accepted for the reference's signature (the b200 path copies each table to HBM once).
+    table_dtype: how the b200 path keeps the tables in HBM -- 'f32' (as stored), or 'f16' / 'bf16'
+    (half the bytes; see quantize_table for the values it then uses)"""
+    if table_dtype not in TABLE_DTYPES:
+        raise ValueError("table_dtype must be 'f32', 'f16' or 'bf16'")
     files = glob.glob(os.path.join(store_dir, "bd_*.npz"))
     if not files:
         raise FileNotFoundError("no bd_*.npz in %s" % store_dir)
@@ -84,7 +92,52 @@ def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False):
             tables = list(ex.map(lambda f: read_npz_member(f, "T.npy"), files))
     return RedshiftStore(s=np.array(s), alpha_lo=np.array(alo), alpha_hi=np.array(ahi), beta=list(beta),
                          delta=list(delta), tau_idx=tau[0], tables=tables,
-                         n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]))
+                         n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]), table_dtype=table_dtype)
+
+
+def with_table_dtype(store, table_dtype):
+    """the same store (host tables shared) kept in HBM as table_dtype ('f32', 'f16', 'bf16')"""
+    import copy
+    if table_dtype not in TABLE_DTYPES:
+        raise ValueError("table_dtype must be 'f32', 'f16' or 'bf16'")
+    out = copy.copy(store)
+    out.__dict__.pop("_b200_token", None)     # a store object of its own
+    out.table_dtype = table_dtype
+    if hasattr(out, "device_tokens"):
+        out.device_tokens = {}
+    return out
+
+
+def _bf16_round(x):
+    """float32 -> nearest bfloat16 (ties to even), returned as float32"""
+    u = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def quantize_table(T, table_dtype):
+    """(values, scale): the float32 values the b200 path uses for one node table kept as
+    table_dtype, and the node's scale -- the device quantizer restated on the host, bit for bit.
+    f16: element = round(T / scale) to float16 (nearest, ties to even), scale = 2^(e - 15) with
+    max|T| = f 2^e, f in [0.5, 1), so max|T| / scale lies in [2^14, 2^15); value = element * scale.
+    bf16: element = round(T) to bfloat16, scale 1.  f32: T itself."""
+    T = np.asarray(T, np.float32)
+    if table_dtype == "f32":
+        return T, 1.0
+    if table_dtype == "bf16":
+        return _bf16_round(T), 1.0
+    if table_dtype != "f16":
+        raise ValueError("table_dtype must be 'f32', 'f16' or 'bf16'")
+    amax = float(np.abs(T).max()) if T.size else 0.0
+    if not np.isfinite(amax):
+        raise ValueError("node table holds a non-finite value")
+    if amax > 0:
+        _, e = np.frexp(np.float32(amax))
+        scale = np.float32(np.ldexp(np.float32(1.0), int(e) - 15))
+    else:
+        scale = np.float32(1.0)
+    h = (T * np.float32(1.0 / scale)).astype(np.float16)
+    return (h.astype(np.float32) * scale).astype(np.float32), float(scale)
 
 
 def store_grid(store):
@@ -99,13 +152,14 @@ def store_grid(store):
 
 def upload_store(store, ctx):
     """copy the store's tables into the context's HBM once (skipped if this store is already resident)"""
-    token = _lib.token_of(store)
+    token = (_lib.token_of(store), getattr(store, "table_dtype", "f32"))
     if ctx.store_token == token:
         return
     gen = getattr(store, "generator", None)
     shape = tuple(store.spec.shape) if gen is not None else tuple(np.asarray(store.tables[0]).shape)
     beta0, dbeta, delta0, ddelta = store_grid(store)
-    ctx.store_init(len(store.tables), shape, store.tau_idx, beta0, dbeta, delta0, ddelta)
+    dtype = TABLE_DTYPES[getattr(store, "table_dtype", "f32")]
+    ctx.store_init(len(store.tables), shape, store.tau_idx, beta0, dbeta, delta0, ddelta, dtype)
     for k, T in enumerate(store.tables):
         if gen is not None and T is None:
             M, P, Q, S, seed = gen

@@ -299,8 +299,9 @@ class MemoryStore:
     """a store held in memory with the fields of the reference's RedshiftStore
     (exmarg/search/store.py:171-181)"""
 
-    def __init__(self, spec, s_nodes, seed, tables=None, n_max=120):
+    def __init__(self, spec, s_nodes, seed, tables=None, n_max=120, table_dtype="f32"):
         self.spec = spec
+        self.table_dtype = table_dtype
         self.s = np.asarray(s_nodes, float)
         self.alpha_lo = np.full(self.s.size, ALPHA[0])
         self.alpha_hi = np.full(self.s.size, ALPHA[-1])
