@@ -194,7 +194,10 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
     *pS = s;
 }
 
-#define TPL 4   // consecutive taps per lane (in groups of GRP); a warp chunk is 32 * TPL taps
+#ifndef EXM_TPL
+#define EXM_TPL 4
+#endif
+#define TPL EXM_TPL   // consecutive taps per lane (in groups of GRP); a warp chunk is 32 * TPL taps
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
