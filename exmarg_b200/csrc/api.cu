@@ -734,8 +734,9 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
     exm_ensure(ctx, sl.hist, (EXM_HB_N + 256) * sizeof(int));
     exm_ensure(ctx, sl.win, (1 + EXM_MAX_NODES) * sizeof(int));
     exm_ensure(ctx, sl.cnt, (size_t)rs.rc * EXM_NPAIR * (nmc + 1) * sizeof(int));
-    exm_ensure(ctx, sl.desc, (size_t)rs.rc * nmc * rs.nwalk * sizeof(uint4));
-    exm_ensure(ctx, sl.tside, (size_t)rs.rc * nmc * rs.nwalk * sizeof(int32_t));
+    const size_t pitch = (size_t)exm_desc_pitch((long long)nmc * rs.nwalk);
+    exm_ensure(ctx, sl.desc, (size_t)rs.rc * pitch * sizeof(uint4));
+    exm_ensure(ctx, sl.tside, (size_t)rs.rc * pitch * sizeof(int32_t));
     exm_ensure(ctx, sl.part, (size_t)(ctx->nn + 1) * ctx->ntau * ctx->nm * sizeof(double));
     exm_ensure(ctx, sl.lnl, (size_t)ctx->nm * sizeof(double));
     exm_ensure(ctx, sl.lnb, sizeof(double));
@@ -1185,8 +1186,9 @@ extern "C" int exm_node_values(exm_ctx *ctx, double *lamN_out)
     rs.rc = (int)std::max<size_t>(1, std::min<size_t>((size_t)ctx->ntau, ((size_t)8 << 30) / per_lag));
     exm_slot &sl = ctx->slot;
     exm_ensure(ctx, sl.cnt, (size_t)rs.rc * EXM_NPAIR * (ctx->nm + 1) * sizeof(int));
-    exm_ensure(ctx, sl.desc, (size_t)rs.rc * ctx->nm * rs.nwalk * sizeof(uint4));
-    exm_ensure(ctx, sl.tside, (size_t)rs.rc * ctx->nm * rs.nwalk * sizeof(int32_t));
+    const size_t pitch = (size_t)exm_desc_pitch((long long)ctx->nm * rs.nwalk);
+    exm_ensure(ctx, sl.desc, (size_t)rs.rc * pitch * sizeof(uint4));
+    exm_ensure(ctx, sl.tside, (size_t)rs.rc * pitch * sizeof(int32_t));
     exm_ensure(ctx, sl.part, (size_t)(ctx->nn + 1) * ctx->ntau * ctx->nm * sizeof(double));
     EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
     ChunkInfo ci{0, ctx->nm, rs.nwalk, rs.use_sel, rs.lw};

@@ -194,10 +194,7 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
     *pS = s;
 }
 
-#ifndef EXM_TPL
-#define EXM_TPL 4
-#endif
-#define TPL EXM_TPL   // consecutive taps per lane (in groups of GRP); a warp chunk is 32 * TPL taps
+#define TPL EXM_TPL   // consecutive taps per lane (in groups of GRP); a warp chunk is EXM_DCH taps
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
@@ -225,16 +222,18 @@ __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, flo
 // GRP taps: decode, window interpolation for all of them (no branch between the shared loads),
 // the exact float64 value for the rare taps outside the window, then the merges
 template <bool BND, int GRP, typename TE>
-__device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, const uint4 *q, int j, int end, int &cT,
-                                          float &cB, float &cE, float &cS, int &fT, float &fB, float &fE, float &fS,
-                                          unsigned &n_slow)
+__device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, const uint4 *q, int j, int pj, int beg,
+                                          int end, int &cT, float &cB, float &cE, float &cS, int &fT, float &fB,
+                                          float &fE, float &fS, unsigned &n_slow)
 {
+    // j: sorted position of the group's first tap (taps j .. j + GRP - 1 of this lane);
+    // pj: its storage index (tap u of the group at pj + 32 u)
     int t[GRP], o[GRP];
     bool fast[GRP];
     float fbf[GRP], fd[GRP], w[GRP], lwv[GRP], vB[GRP], vE[GRP];
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
-        int tt = (j + u < end) ? (int)(q[u].w >> 19) + c.m_base - c.lo : -1;
+        int tt = (j + u >= beg && j + u < end) ? (int)(q[u].w >> 19) + c.m_base - c.lo : -1;
         if (tt >= c.n) {   // outside the block's templates: report and skip
             atomicOr(a.err, EXM_DEVERR_BOUNDS);
             tt = -1;
@@ -266,7 +265,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         if (t[u] >= 0 && !fast[u]) {
             ++n_slow;
             const int il = (int)(q[u].w >> 19);
-            const int tm = c.tsr[j + u];
+            const int tm = c.tsr[pj + 32 * u];
             int i1 = tm + c.tau0;
             if (i1 >= c.nt) i1 -= c.nt;
             const int gi = il + c.m_base;
@@ -284,13 +283,18 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
 template <bool BND, int GRP, typename TE>
 __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
 {
+    // the warp's sorted positions [beg, end), walked in whole chunks of EXM_DCH (positions outside
+    // [beg, end) masked); lane l takes the chunk's positions l*TPL + i, stored at i*32 + l
     const int lane = threadIdx.x & 31;
+    const int jstart = beg & ~(EXM_DCH - 1);
     uint4 qa[GRP];
-    int jb = beg + TPL * lane;
 #pragma unroll
-    for (int u = 0; u < GRP; ++u) qa[u] = (jb + u < end) ? __ldg(c.descr + jb + u) : make_uint4(0u, 0u, 0u, 0u);
-    for (int j0 = beg; j0 < end; j0 += 32 * TPL) {
-        jb = j0 + TPL * lane;
+    for (int u = 0; u < GRP; ++u) {
+        const int jl = jstart + TPL * lane + u;
+        qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int j0 = jstart; j0 < end; j0 += EXM_DCH) {
+        const int jb = j0 + TPL * lane;
         int cT = -1, fT = -1;
         float cB = -1e30f, cE = 0.f, cS = 0.f, fB = -1e30f, fE = 0.f, fS = 0.f;
 #pragma unroll
@@ -299,13 +303,19 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
 #pragma unroll
             for (int u = 0; u < GRP; ++u) cur[u] = qa[u];
             // the next group of descriptors (this lane's next group, or the next chunk's first)
-            const int jn = (g + 1 < TPL / GRP) ? jb + (g + 1) * GRP : jb + 32 * TPL;
-            if (g + 1 < TPL / GRP || j0 + 32 * TPL < end) {
+            const bool same = g + 1 < TPL / GRP;
+            const int jn0 = same ? j0 : j0 + EXM_DCH;
+            const int gn = same ? (g + 1) * GRP : 0;
+            if (same || j0 + EXM_DCH < end) {
 #pragma unroll
-                for (int u = 0; u < GRP; ++u)
-                    qa[u] = (jn + u < end) ? __ldg(c.descr + jn + u) : make_uint4(0u, 0u, 0u, 0u);
+                for (int u = 0; u < GRP; ++u) {
+                    const int jl = jn0 + TPL * lane + gn + u;
+                    qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jn0 + 32 * (gn + u) + lane)
+                                                    : make_uint4(0u, 0u, 0u, 0u);
+                }
             }
-            tap_group<BND, GRP, TE>(a, c, cur, jb + g * GRP, end, cT, cB, cE, cS, fT, fB, fE, fS, n_slow);
+            tap_group<BND, GRP, TE>(a, c, cur, jb + g * GRP, j0 + 32 * g * GRP + lane, beg, end, cT, cB, cE, cS, fT,
+                                    fB, fE, fS, n_slow);
         }
         // the first closed template of lane l + 1 continues lane l's last one, or is lane l + 1's alone
         const int nT = __shfl_down_sync(0xffffffffu, fT, 1);
@@ -321,10 +331,10 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
     }
 }
 
-// the template of descriptor j (block-local), or -1
+// the template of the descriptor at sorted position j (block-local), or -1
 __device__ __forceinline__ int desc_template(const RunCtx &c, int j)
 {
-    return (int)(__ldg(&c.descr[j].w) >> 19) + c.m_base - c.lo;
+    return (int)(__ldg(&c.descr[exm_desc_phys(j)].w) >> 19) + c.m_base - c.lo;
 }
 
 // fold the warps' edge partials into the accumulators: one warp, lane w holding warp w's first (F)
@@ -376,8 +386,14 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
                                            unsigned &n_slow)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w0 = beg + (int)((long long)(end - beg) * warp / NW);
-    const int w1 = beg + (int)((long long)(end - beg) * (warp + 1) / NW);
+    // whole storage chunks per warp, as evenly as they divide (the first and last may be partial).
+    // The warps with work are a prefix: the edge fold merges equal templates of neighbouring lanes
+    // only, so an empty warp between two that share a template would let both update its
+    // accumulator at once.
+    const int cb = beg / EXM_DCH, nc = (end + EXM_DCH - 1) / EXM_DCH - cb;
+    const int q = nc / NW, rem = nc % NW;
+    const int c0 = cb + warp * q + min(warp, rem), c1 = c0 + q + (warp < rem ? 1 : 0);
+    const int w0 = max(beg, c0 * EXM_DCH), w1 = min(end, c1 * EXM_DCH);
     float *e = edge + 8 * warp;
     int tF = -1, tL = -1;
     if (w0 < w1) {
@@ -620,7 +636,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.err = (unsigned *)sl.dev_err.p;
     a.stats = (unsigned long long *)ctx->d_stats.p;
     a.tstride = (long long)ctx->tstride;
-    a.per_lag = (long long)ci.nmc * ci.nwalk;
+    a.per_lag = exm_desc_pitch((long long)ci.nmc * ci.nwalk);   // storage stride of a lag's descriptors
     a.nn = ctx->nn;
     a.ntau = ctx->ntau;
     a.nphif = ctx->nphif;

@@ -43,6 +43,27 @@ inline size_t exm_dtype_bytes(int dtype) { return dtype == EXM_DTYPE_F32 ? 4 : 2
 inline int exm_dtype_wd(int dtype) { return dtype == EXM_DTYPE_F32 ? EXM_WD : EXM_WD16; }
 inline int exm_dtype_calign(int dtype) { return dtype == EXM_DTYPE_F32 ? 4 : 8; }
 #define EXM_TCH 2048        // templates per gather block
+
+// Tap descriptors of one lag, sorted by (plane pair, template), are stored in chunks of
+// EXM_DCH = 32 * EXM_TPL.  The gather's lane l takes the consecutive taps l*TPL .. l*TPL+TPL-1
+// of a chunk (so equal templates meet in registers), and they are stored lane-interleaved --
+// tap i of lane l at i*32 + l -- so that every load instruction of a warp reads 32 consecutive
+// descriptors (512 bytes) instead of 32 scattered cache lines.
+#ifndef EXM_TPL
+#define EXM_TPL 4
+#endif
+#define EXM_DCH (32 * EXM_TPL)
+static_assert((EXM_TPL & (EXM_TPL - 1)) == 0, "taps per lane must be a power of two");
+
+// storage index of the descriptor at sorted position j (within its lag)
+__host__ __device__ __forceinline__ long long exm_desc_phys(long long j)
+{
+    const long long q = j & (EXM_DCH - 1);
+    return (j - q) + (q % EXM_TPL) * 32 + q / EXM_TPL;
+}
+
+// descriptors per lag as stored: whole chunks
+inline long long exm_desc_pitch(long long per_lag) { return (per_lag + EXM_DCH - 1) / EXM_DCH * EXM_DCH; }
 #define EXM_MAX_CHUNK 8192  // templates per pass (13-bit template field of a descriptor)
 #define EXM_MAX_NODES 64
 #define EXM_HB_LO (-1024)   // beta-hat histogram covers [-1024, 1024)

@@ -26,6 +26,7 @@ struct TapArgs {
     TapGeom g;
     int nmc, nwalk, use_sel, r0, want_hb;
     long long per_lag;    // nmc * nwalk
+    long long pitch;      // descriptors stored per lag (whole chunks, exm_desc_pitch)
 };
 
 __device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t, int &flag)
@@ -195,8 +196,8 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     for (int rl = 0; rl < rc; ++rl) {
         const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
         const int *off = a.cnt + (long long)rl * EXM_NPAIR * (a.nmc + 1);
-        uint4 *desc = a.desc + (long long)rl * a.per_lag;
-        int32_t *tside = a.tside + (long long)rl * a.per_lag;
+        uint4 *desc = a.desc + (long long)rl * a.pitch;
+        int32_t *tside = a.tside + (long long)rl * a.pitch;
         __syncthreads();
         for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) base[q] = off[q * (a.nmc + 1) + i];
         for (int k0 = 0; k0 < a.nwalk; k0 += blockDim.x) {
@@ -234,8 +235,9 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
                 d.y = __float_as_uint(fd);
                 d.z = __float_as_uint(w) | ((unsigned)flag << 31);
                 d.w = ((unsigned)i << 19) | ((unsigned)d0 << 11) | ((unsigned)ib & 0x7FFu);
-                desc[pos] = d;
-                tside[pos] = t;
+                const long long ph = exm_desc_phys(pos);
+                desc[ph] = d;
+                tside[ph] = t;
             }
             __syncthreads();
         }
@@ -303,6 +305,7 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     a.r0 = r0;
     a.want_hb = first_chunk_of_lags ? 1 : 0;
     a.per_lag = (long long)ci.nmc * ci.nwalk;
+    a.pitch = exm_desc_pitch(a.per_lag);
     if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
     EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
     const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int)) : 0;
