@@ -576,9 +576,10 @@ struct GatherCfg {
 static const GatherCfg kGatherCfgs[] = {{16, 4}, {16, 2}, {24, 2}, {32, 2}, {32, 1}};
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
-template <int NW, int GRP, typename TE>
+template <int NW, int GRP0, typename TE>
 static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
 {
+    constexpr int GRP = GRP0 < TPL ? GRP0 : TPL;   // a register group never exceeds a lane's taps
     exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP, TE>, smem);
     k_gather_planes<NW, GRP, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
 }
