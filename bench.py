@@ -363,7 +363,7 @@ def run_b200(args):
     elif not args.no_tune:
         best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
         tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:5]],
-                "shapes": ["16w x4", "16w x2", "24w x2", "32w x2", "32w x1"]}
+                "shapes": list(_lib.GATHER_SHAPES)}
     ctx.timing(True)
     if pg:
         pg.barrier()

@@ -195,6 +195,10 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
 }
 
 #define TPL EXM_TPL   // consecutive taps per lane (in groups of GRP); a warp chunk is EXM_DCH taps
+#ifndef EXM_GUNROLL
+#define EXM_GUNROLL 2
+#endif
+constexpr int kGroupUnroll = EXM_GUNROLL;   // tap groups of a chunk unrolled in the lane loop
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
@@ -217,6 +221,23 @@ __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, flo
         cS = 0.f;
     }
     lse_merge(cB, cE, cS, vB, vE, t >= 0 ? 1.f : 0.f);
+}
+
+// the exact float64 value of a tap outside the staged window (rare)
+#ifndef EXM_SLOW_INLINE
+#define EXM_SLOW_INLINE __forceinline__
+#endif
+template <bool BND, typename TE>
+__device__ EXM_SLOW_INLINE double slow_tap(const PlaneArgs &a, int il, int tm, int k, int r, int tau0, int m_base, int nt,
+                                        double offb_node, float sc)
+{
+    int i1 = tm + tau0;
+    if (i1 >= nt) i1 -= nt;
+    const int gi = il + m_base;
+    const double offb = (BND ? a.cb[gi] : offb_node) + a.boff[gi];
+    return exm_tap_fp64<TE>(a.L[(long long)il * nt + tm], a.H[(long long)il * nt + i1], offb, r,
+                            (const TE *)a.T + (long long)k * a.tstride, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
+                            a.rdd, a.offd);
 }
 
 // GRP taps: decode, window interpolation for all of them (no branch between the shared loads),
@@ -264,15 +285,8 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
     for (int u = 0; u < GRP; ++u) {
         if (t[u] >= 0 && !fast[u]) {
             ++n_slow;
-            const int il = (int)(q[u].w >> 19);
-            const int tm = c.tsr[pj + 32 * u];
-            int i1 = tm + c.tau0;
-            if (i1 >= c.nt) i1 -= c.nt;
-            const int gi = il + c.m_base;
-            const double offb = (BND ? a.cb[gi] : c.offb_node) + a.boff[gi];
-            const double v = exm_tap_fp64<TE>(a.L[(long long)il * c.nt + tm], a.H[(long long)il * c.nt + i1], offb,
-                                              c.r, (const TE *)a.T + (long long)c.k * a.tstride, c.sc, a.nphif, a.nb,
-                                              a.nd, a.ndp, a.rph, a.rdb, a.rdd, a.offd);
+            const double v = slow_tap<BND, TE>(a, (int)(q[u].w >> 19), c.tsr[pj + 32 * u], c.k, c.r, c.tau0, c.m_base,
+                                               c.nt, c.offb_node, c.sc);
             split_double(v, vB[u], vE[u]);
         }
     }
@@ -297,7 +311,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
         const int jb = j0 + TPL * lane;
         int cT = -1, fT = -1;
         float cB = -1e30f, cE = 0.f, cS = 0.f, fB = -1e30f, fE = 0.f, fS = 0.f;
-#pragma unroll
+#pragma unroll(kGroupUnroll)
         for (int g = 0; g < TPL / GRP; ++g) {
             uint4 cur[GRP];
 #pragma unroll
@@ -419,7 +433,8 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
 }
 
 template <int NW, int GRP, typename TE>
-__global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap, const PlaneArgs a)
+__global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap,
+                                                                const __grid_constant__ PlaneArgs a)
 {
     constexpr int SLOT = slot_elems<TE>();
     constexpr unsigned SLOT_B = slot_bytes<TE>();
@@ -573,7 +588,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{16, 4}, {16, 2}, {24, 2}, {32, 2}, {32, 1}};
+static const GatherCfg kGatherCfgs[] = {{24, 2}, {16, 2}, {24, 1}, {32, 2}, {32, 1}};
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -588,9 +603,9 @@ template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<16, 4, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
     case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
-    case 2: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
     case 3: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
     default: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
     }

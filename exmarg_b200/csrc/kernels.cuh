@@ -50,7 +50,7 @@ inline int exm_dtype_calign(int dtype) { return dtype == EXM_DTYPE_F32 ? 4 : 8; 
 // tap i of lane l at i*32 + l -- so that every load instruction of a warp reads 32 consecutive
 // descriptors (512 bytes) instead of 32 scattered cache lines.
 #ifndef EXM_TPL
-#define EXM_TPL 4
+#define EXM_TPL 16
 #endif
 #define EXM_DCH (32 * EXM_TPL)
 static_assert((EXM_TPL & (EXM_TPL - 1)) == 0, "taps per lane must be a power of two");
