@@ -732,7 +732,7 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
     exm_ensure(ctx, sl.rej, (1 + EXM_MAX_REJ) * sizeof(int));
     exm_ensure(ctx, sl.sel, std::max<size_t>(1, rs.use_sel ? nmc * rs.nwalk : 1) * sizeof(int32_t));
     exm_ensure(ctx, sl.hist, (EXM_HB_N + 256) * sizeof(int));
-    exm_ensure(ctx, sl.win, (1 + EXM_MAX_NODES) * sizeof(int));
+    exm_ensure(ctx, sl.win, (2 + EXM_MAX_NODES) * sizeof(int));
     exm_ensure(ctx, sl.cnt, (size_t)rs.rc * EXM_NPAIR * (nmc + 1) * sizeof(int));
     const size_t pitch = (size_t)exm_desc_pitch((long long)nmc * rs.nwalk);
     exm_ensure(ctx, sl.desc, (size_t)rs.rc * pitch * sizeof(uint4));

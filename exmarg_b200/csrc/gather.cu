@@ -161,10 +161,12 @@ struct RunCtx {
     const void *s0, *s1;        // the staged windows of planes p and p + 1 (element type TE)
     float sc;                   // the node's scale (16-bit tables)
     float *aB, *aE, *aS;        // accumulators of the run's templates, index t - lo
-    const int *bci;             // boundary runs: per-template integer offset (index t - lo)
-    const float *bcf;           //                and fraction
+    const int *bsh;             // boundary runs: per-template window-row shift (index t - lo)
+    const float *bcf;           //                and beta fraction
     const int *bnode;           // boundary runs: which templates have their boundary here
-    int lo, m_base, n, R0, C0, cki, k, r, tau0, nt;
+    int lo, m_base, n, k, r, tau0, nt;
+    int sh;                     // window row of a tap = rb0 + carry + sh (regular runs)
+    int up, edge;               // fast path: row <= up, and not (row == edge with beta at the clamp)
     float ckf, lw;
     double offb_node;           // (ln s_k - beta0)/dbeta, regular runs
     int tF, tL;                 // the templates at the two ends of this warp's taps (may be shared with
@@ -266,17 +268,15 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         fd[u] = __uint_as_float(q[u].y);
         w[u] = __uint_as_float(q[u].z & 0x7FFFFFFFu);
         lwv[u] = (q[u].z >> 31) ? c.lw : 0.f;
-        const int d0 = (int)((q[u].w >> 11) & 0xFFu);
-        const int ibh = ((int)(q[u].w << 21)) >> 21;
+        const int rd = (int)((q[u].w >> 11) & 0xFFu);      // window column (255: outside)
+        const int rb0 = ((int)(q[u].w << 21)) >> 21;        // beta-hat row from the window origin
         const float sfr = fb + (BND ? c.bcf[ts] : c.ckf);
         const int cy = sfr >= 1.f;
         fbf[u] = cy ? sfr - 1.f : sfr;
-        const int b0 = ibh + (BND ? c.bci[ts] : c.cki) + cy;
-        const int rb = b0 - c.R0, rd = d0 - c.C0;
+        const int rb = rb0 + cy + (BND ? c.bsh[ts] : c.sh);   // this node's window row
         constexpr int WD = TabElem<TE>::wd;
-        fast[u] = (unsigned)rb <= (unsigned)(EXM_WB - 2) && (unsigned)rd <= (unsigned)(WD - 2) &&
-                  b0 <= a.nb - 2 && !(b0 == a.nb - 2 && fbf[u] > 0.999999f);
-        o[u] = min(max(rb, 0), EXM_WB - 2) * WD + min(max(rd, 0), WD - 2);
+        fast[u] = (unsigned)rb <= (unsigned)c.up && rd <= WD - 2 && !(rb == c.edge && fbf[u] > 0.999999f);
+        o[u] = fast[u] ? rb * WD + rd : 0;
     }
 #pragma unroll
     for (int u = 0; u < GRP; ++u)
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     float *aE = aB + tch, *aS = aE + tch;
     float *bB = aS + tch, *bE = bB + tch, *bS = bE + tch;
     float *bcf = bS + tch;
-    int *bci = (int *)(bcf + tch);
+    int *bsh = (int *)(bcf + tch);
     __shared__ float edge[2][8 * NW];   // per warp: F partial + id, L partial + id (regular, boundary)
 
     // block -> (lag, node, template chunk), lags outermost so the blocks of one lag run together
@@ -467,6 +467,10 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         bl_sh[1] = 0;
     }
     __syncthreads();
+    // the node's window: column C0, first row R0 = Rh + cki clamped to the table; a tap's window row
+    // is its beta-hat row from Rh (in the descriptor), plus the carry of the node's beta fraction, plus sh
+    const int C0 = a.win[0], R0 = a.win[1 + k], Rh = a.win[1 + EXM_MAX_NODES];
+    const int sh = Rh + a.cki[k] - R0;
     for (int j = tid; j < n; j += NW * 32) {
         aB[j] = -1e30f;
         aE[j] = 0.f;
@@ -477,13 +481,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             bS[j] = 0.f;
             const double cbv = a.cb[lo + j];
             const double f = floor(cbv);
-            bci[j] = (int)f;
+            bsh[j] = (int)f - a.cki[k] + sh;
             bcf[j] = (float)(cbv - f);
             atomicMin(&bl_sh[0], j);
             atomicMax(&bl_sh[1], j + 1);
         }
     }
-    const int C0 = a.win[0], R0 = a.win[1 + k];
     if (tid == 0) {
         for (int s = 0; s < 3; ++s) mbar_init(&mbar[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -501,15 +504,15 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     RunCtx rc;
     rc.descr = a.desc + (long long)rl * a.per_lag;
     rc.tsr = a.tside + (long long)rl * a.per_lag;
-    rc.bci = bci;
+    rc.bsh = bsh;
     rc.bcf = bcf;
     rc.bnode = a.bnode;
     rc.lo = lo;
     rc.m_base = a.m_base;
     rc.n = n;
-    rc.R0 = R0;
-    rc.C0 = C0;
-    rc.cki = a.cki[k];
+    rc.sh = sh;
+    rc.up = min(EXM_WB - 2, a.nb - 2 - R0);
+    rc.edge = a.nb - 2 - R0;
     rc.ckf = a.ckf[k];
     rc.sc = a.tsc[k];
     rc.k = k;

@@ -6,7 +6,12 @@
 // packed into 16 bytes:
 //   x = fb (float, fraction of beta-hat), y = fd (float, fraction of Delta),
 //   z = w (float, weight of plane p + 1) | bit 31: the time is a random draw,
-//   w = template (13 bits) << 19 | d0 (8 bits) << 11 | floor(beta-hat) (11 bits, signed).
+//   w = template (13 bits) << 19 | rd (8 bits) << 11 | rb0 (11 bits, signed),
+// with the staging windows already placed (k_windows runs between the count and the
+// scatter): rd = d0 - C0, the column inside every node's window (255: outside, the
+// exact path), and rb0 = floor(beta-hat) - Rh, the row relative to the window row
+// origin in beta-hat; node k's window row of the tap is then rb0 + carry + a constant
+// of the node, so the gather adds only the node's part.
 // For each lag the descriptors are counting-sorted by (p, template), so every node's
 // gather block reads, for each plane pair it has staged, one contiguous run per warp.
 // A second array holds each descriptor's time index for the exact slow path.
@@ -27,6 +32,8 @@ struct TapArgs {
     int nmc, nwalk, use_sel, r0, want_hb;
     long long per_lag;    // nmc * nwalk
     long long pitch;      // descriptors stored per lag (whole chunks, exm_desc_pitch)
+    const int *win;       // window origins (k_windows): [0] column C0, [1 + EXM_MAX_NODES] beta-hat row Rh
+    int wd;               // window columns
 };
 
 __device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t, int &flag)
@@ -193,6 +200,7 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     wc.flag = wc.t + TAP_CACHE;
     load_walk(a, i, L, wc);
     const unsigned lt = (1u << lane) - 1u;
+    const int C0 = a.win[0], Rh = a.win[1 + EXM_MAX_NODES];
     for (int rl = 0; rl < rc; ++rl) {
         const int tau0 = ((a.tau[a.r0 + rl] % nt) + nt) % nt;
         const int *off = a.cnt + (long long)rl * EXM_NPAIR * (a.nmc + 1);
@@ -234,7 +242,12 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
                 d.x = __float_as_uint(fb);
                 d.y = __float_as_uint(fd);
                 d.z = __float_as_uint(w) | ((unsigned)flag << 31);
-                d.w = ((unsigned)i << 19) | ((unsigned)d0 << 11) | ((unsigned)ib & 0x7FFu);
+                int rd = d0 - C0, rb0 = ib - Rh;
+                if ((unsigned)rd > (unsigned)(a.wd - 2) || rb0 < -1024 || rb0 > 1023) {
+                    rd = 255;   // outside every node's window: the exact path
+                    rb0 = 0;
+                }
+                d.w = ((unsigned)i << 19) | ((unsigned)rd << 11) | ((unsigned)rb0 & 0x7FFu);
                 const long long ph = exm_desc_phys(pos);
                 desc[ph] = d;
                 tside[ph] = t;
@@ -244,8 +257,8 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     }
 }
 
-// staging-window origins: column C0 (a multiple of calign elements, 16 bytes) and, per node,
-// the first beta row; wd columns per window
+// staging-window origins: column C0 (a multiple of calign elements, 16 bytes), per node the
+// first beta row, and the beta-hat row origin Rh they derive from; wd columns per window
 __global__ void k_windows(const int *hist_b, const int *hist_d, const int *cki, int nn, int nb, int nd, int ndp,
                           int wd, int calign, int *win)
 {
@@ -276,6 +289,7 @@ __global__ void k_windows(const int *hist_b, const int *hist_d, const int *cki, 
             r0 = max(0, min(r0, nb - EXM_WB));
             win[1 + k] = r0;
         }
+        win[1 + EXM_MAX_NODES] = rh;
     }
 }
 
@@ -311,11 +325,13 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int)) : 0;
     exm_allow_smem(ctx, (const void *)k_tap_count, wsm);
     exm_allow_smem(ctx, (const void *)k_tap_scatter, wsm);
+    a.win = (const int *)sl.win.p;
+    a.wd = exm_dtype_wd(ctx->dtype);
     k_tap_count<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_tap_scan<<<rc, 1024, 0, ctx->stream>>>(a.cnt, ci.nmc);
-    k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           exm_dtype_wd(ctx->dtype), exm_dtype_calign(ctx->dtype), (int *)sl.win.p);
+    k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
     EXM_CUDA(cudaGetLastError());
     ctx->launches += 4;
 }
