@@ -432,22 +432,38 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     if (w0 < w1) process_run<BND, GRP, TE>(a, c, w0, w1, n_slow);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Warp NW - 1 is the producer: it stages the planes with TMA and, once every consumer warp has
+// arrived on the pair's "done" barrier, folds that pair's edge partials and refills the slot of
+// the plane no longer needed.  The NW - 1 consumer warps walk the pairs without a block barrier:
+// a fast warp runs at most one pair ahead of the slowest (pair p + 2 needs plane p + 3, staged
+// only after pair p is done everywhere).  So at most two consecutive pairs are in flight, and the
+// consumers' accumulators alternate with the pair's parity (two warps in different pairs never
+// share a word), while the producer folds edges into a third set of its own.
 template <int NW, int GRP, typename TE>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap,
                                                                 const __grid_constant__ PlaneArgs a)
 {
+    constexpr int NC = NW - 1;   // consumer warps
     constexpr int SLOT = slot_elems<TE>();
     constexpr unsigned SLOT_B = slot_bytes<TE>();
     extern __shared__ __align__(1024) unsigned char smem[];
     TE *win = (TE *)smem;
-    uint64_t *mbar = (uint64_t *)(smem + 3 * SLOT_B);
-    float *aB = (float *)(smem + 3 * SLOT_B + 64);
+    uint64_t *full = (uint64_t *)(smem + 3 * SLOT_B);   // [3] plane staged in slot s
+    uint64_t *done = full + 3;                          // [2] every consumer is done with a pair (parity)
     const int tch = a.tch;
-    float *aE = aB + tch, *aS = aE + tch;
-    float *bB = aS + tch, *bE = bB + tch, *bS = bE + tch;
-    float *bcf = bS + tch;
+    // accumulator sets of 3 x tch floats (B, E, S): regular pairs of parity 0 / 1, regular edges
+    // (producer), boundary pairs of parity 0 / 1, boundary edges
+    float *acc = (float *)(smem + 3 * SLOT_B + 64);
+    float *bcf = acc + 18 * tch;
     int *bsh = (int *)(bcf + tch);
-    __shared__ float edge[2][8 * NW];   // per warp: F partial + id, L partial + id (regular, boundary)
+    __shared__ float edge[2][2][8 * NC];   // [pair parity][regular, boundary]: per warp F and L partials + ids
+    __shared__ int bl_sh[2];
+    __shared__ unsigned bad_sh;
 
     // block -> (lag, node, template chunk), lags outermost so the blocks of one lag run together
     const int c_idx = blockIdx.x % a.nch;
@@ -458,13 +474,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     const int hi = min(hi0, lo + tch);
     if (lo >= hi) return;
     const int n = hi - lo;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // accumulators; the boundary range [blo, bhi) of the templates whose lowest point is node k
-    __shared__ int bl_sh[2];
     if (tid == 0) {
         bl_sh[0] = n;
         bl_sh[1] = 0;
+        bad_sh = 0;
     }
     __syncthreads();
     // the node's window: column C0, first row R0 = Rh + cki clamped to the table; a tap's window row
@@ -472,13 +487,13 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     const int C0 = a.win[0], R0 = a.win[1 + k], Rh = a.win[1 + EXM_MAX_NODES];
     const int sh = Rh + a.cki[k] - R0;
     for (int j = tid; j < n; j += NW * 32) {
-        aB[j] = -1e30f;
-        aE[j] = 0.f;
-        aS[j] = 0.f;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            acc[(3 * q) * tch + j] = -1e30f;
+            acc[(3 * q + 1) * tch + j] = 0.f;
+            acc[(3 * q + 2) * tch + j] = 0.f;
+        }
         if (a.bnode[lo + j] == k) {
-            bB[j] = -1e30f;
-            bE[j] = 0.f;
-            bS[j] = 0.f;
             const double cbv = a.cb[lo + j];
             const double f = floor(cbv);
             bsh[j] = (int)f - a.cki[k] + sh;
@@ -488,79 +503,100 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         }
     }
     if (tid == 0) {
-        for (int s = 0; s < 3; ++s) mbar_init(&mbar[s], 1);
+        for (int s = 0; s < 3; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < 2; ++s) mbar_init(&done[s], NC * 32);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     const int blo = bl_sh[0], bhi = bl_sh[1];
-    if (tid == 0) {
-        tma_load_plane(&tmap, &mbar[0], win, C0, R0, 0, r, k, SLOT_B);
-        tma_load_plane(&tmap, &mbar[1], win + SLOT, C0, R0, 1, r, k, SLOT_B);
-    }
-    int issued = 2;
-
-    const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
-    const int nt = a.nt;
-    RunCtx rc;
-    rc.descr = a.desc + (long long)rl * a.per_lag;
-    rc.tsr = a.tside + (long long)rl * a.per_lag;
-    rc.bsh = bsh;
-    rc.bcf = bcf;
-    rc.bnode = a.bnode;
-    rc.lo = lo;
-    rc.m_base = a.m_base;
-    rc.n = n;
-    rc.sh = sh;
-    rc.up = min(EXM_WB - 2, a.nb - 2 - R0);
-    rc.edge = a.nb - 2 - R0;
-    rc.ckf = a.ckf[k];
-    rc.sc = a.tsc[k];
-    rc.k = k;
-    rc.r = r;
-    rc.tau0 = ((a.tau[r] % nt) + nt) % nt;
-    rc.nt = nt;
-    rc.lw = a.lw;
-    rc.offb_node = a.ckd[k];
-    const int base_i = lo - a.m_base;   // chunk-local index of template lo
-
     unsigned n_slow = 0, n_bnd = 0;
-    bool ok = mbar_wait(&mbar[0], 0, a.err);
-    for (int p = 0; p < EXM_NPAIR; ++p) {
-        if (p > 0) {
-            __syncthreads();   // every warp is done with plane p - 1: its slot can be refilled,
-            if (tid < 32) {    // and the edge partials of that pair go into the accumulators
-                fold_edges(edge[0], NW, aB, aE, aS, n);
-                if (blo < bhi) fold_edges(edge[1], NW, bB, bE, bS, n);
+
+    if (warp == NC) {
+        // ---------------------------------------------------------------- producer
+        int issued = 0;
+        if (lane == 0)
+            for (int q = 0; q < 3 && q < a.nphif; ++q)
+                tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
+        issued = min(3, a.nphif);
+        bool ok = true;
+        for (int p = 0; p < EXM_NPAIR; ++p) {
+            ok = ok && __all_sync(0xffffffffu, mbar_wait(&done[p & 1], (p >> 1) & 1, a.err));
+            if (!ok) break;
+            fold_edges(edge[p & 1][0], NC, acc + 6 * tch, acc + 7 * tch, acc + 8 * tch, n);
+            if (blo < bhi) fold_edges(edge[p & 1][1], NC, acc + 15 * tch, acc + 16 * tch, acc + 17 * tch, n);
+            __syncwarp();
+            // plane p is no longer needed anywhere: its slot takes plane p + 3
+            if (p + 3 < a.nphif) {
+                if (lane == 0) tma_load_plane(&tmap, &full[p % 3], win + (p % 3) * SLOT, C0, R0, p + 3, r, k, SLOT_B);
+                ++issued;
             }
-            __syncthreads();
         }
-        if (tid == 0 && ok && p + 2 < a.nphif) {
-            const int q = p + 2;
-            tma_load_plane(&tmap, &mbar[q % 3], win + (q % 3) * SLOT, C0, R0, q, r, k, SLOT_B);
-            ++issued;
+        if (!ok) {
+            if (lane == 0) {
+                atomicOr(&bad_sh, 1u);
+                // drain: the newest copy of each slot completes after the older ones of that slot (bounded)
+                for (int q = max(0, issued - 3); q < issued; ++q) mbar_wait(&full[q % 3], (q / 3) & 1, a.err);
+            }
         }
-        ok = ok && mbar_wait(&mbar[(p + 1) % 3], ((p + 1) / 3) & 1, a.err);
-        if (!ok) continue;
-        rc.s0 = win + (p % 3) * SLOT;
-        rc.s1 = win + ((p + 1) % 3) * SLOT;
-        const int *offp = offr + p * (a.nmc + 1) + base_i;
-        rc.aB = aB;
-        rc.aE = aE;
-        rc.aS = aS;
-        warp_share<false, GRP, NW, TE>(a, rc, offp[0], offp[n], edge[0], n_slow);
-        if (blo < bhi) {
-            rc.aB = bB;
-            rc.aE = bE;
-            rc.aS = bS;
-            const int bb = offp[blo], be = offp[bhi];
-            n_bnd += (lane == 0 && (tid >> 5) == 0) ? (unsigned)(be - bb) : 0u;
-            warp_share<true, GRP, NW, TE>(a, rc, bb, be, edge[1], n_slow);
+    } else {
+        // ---------------------------------------------------------------- consumers
+        const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
+        const int nt = a.nt;
+        RunCtx rc;
+        rc.descr = a.desc + (long long)rl * a.per_lag;
+        rc.tsr = a.tside + (long long)rl * a.per_lag;
+        rc.bsh = bsh;
+        rc.bcf = bcf;
+        rc.bnode = a.bnode;
+        rc.lo = lo;
+        rc.m_base = a.m_base;
+        rc.n = n;
+        rc.sh = sh;
+        rc.up = min(EXM_WB - 2, a.nb - 2 - R0);
+        rc.edge = a.nb - 2 - R0;
+        rc.ckf = a.ckf[k];
+        rc.sc = a.tsc[k];
+        rc.k = k;
+        rc.r = r;
+        rc.tau0 = ((a.tau[r] % nt) + nt) % nt;
+        rc.nt = nt;
+        rc.lw = a.lw;
+        rc.offb_node = a.ckd[k];
+        const int base_i = lo - a.m_base;   // chunk-local index of template lo
+        bool ok = true;
+        for (int p = 0; p < EXM_NPAIR; ++p) {
+            // warp-uniform: the lanes go on to shuffles together
+            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err));
+            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err));
+            if (ok) {
+                rc.s0 = win + (p % 3) * SLOT;
+                rc.s1 = win + ((p + 1) % 3) * SLOT;
+                const int *offp = offr + p * (a.nmc + 1) + base_i;
+                float *A = acc + 3 * (p & 1) * tch;
+                rc.aB = A;
+                rc.aE = A + tch;
+                rc.aS = A + 2 * tch;
+                warp_share<false, GRP, NC, TE>(a, rc, offp[0], offp[n], edge[p & 1][0], n_slow);
+                if (blo < bhi) {
+                    float *Bs = acc + (9 + 3 * (p & 1)) * tch;
+                    rc.aB = Bs;
+                    rc.aE = Bs + tch;
+                    rc.aS = Bs + 2 * tch;
+                    const int bb = offp[blo], be = offp[bhi];
+                    n_bnd += (lane == 0 && warp == 0) ? (unsigned)(be - bb) : 0u;
+                    warp_share<true, GRP, NC, TE>(a, rc, bb, be, edge[p & 1][1], n_slow);
+                }
+            } else if (lane == 0) {   // no work: empty edge slots for the producer
+                for (int b2 = 0; b2 < 2; ++b2) {
+                    float *e = edge[p & 1][b2] + 8 * warp;
+                    e[3] = __int_as_float(-1);
+                    e[7] = __int_as_float(-1);
+                }
+            }
+            __syncwarp();
+            mbar_arrive(&done[p & 1]);
         }
-    }
-    __syncthreads();
-    if (tid < 32 && ok) {
-        fold_edges(edge[0], NW, aB, aE, aS, n);
-        if (blo < bhi) fold_edges(edge[1], NW, bB, bE, bS, n);
+        if (!ok && lane == 0) atomicOr(&bad_sh, 1u);
     }
     if (a.stats) {
         const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);
@@ -570,18 +606,19 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         }
     }
     __syncthreads();
-    // drain: every issued copy has landed before the block exits (bounded)
-    if (!ok && tid == 0) {
-        // the newest copy of each slot completes after the older ones of that slot
-        for (int q = max(0, issued - 3); q < issued; ++q) mbar_wait(&mbar[q % 3], (q / 3) & 1, a.err);
-    }
+    const bool ok = bad_sh == 0;
     for (int j = tid; j < n; j += NW * 32) {
-        const float S = aS[j];
-        const double v = (ok && S > 0.f) ? (double)aB[j] + (double)aE[j] + log((double)S) : -INFINITY;
+        // the three sets of a template: both pair parities and the folded edges
+        float B = acc[j], E = acc[tch + j], S = acc[2 * tch + j];
+        lse_merge(B, E, S, acc[3 * tch + j], acc[4 * tch + j], acc[5 * tch + j]);
+        lse_merge(B, E, S, acc[6 * tch + j], acc[7 * tch + j], acc[8 * tch + j]);
+        const double v = (ok && S > 0.f) ? (double)B + (double)E + log((double)S) : -INFINITY;
         a.part[((long long)k * a.ntau + r) * a.nm_total + lo + j] = v;
         if (j >= blo && j < bhi && a.bnode[lo + j] == k) {
-            const float S2 = bS[j];
-            const double v2 = (ok && S2 > 0.f) ? (double)bB[j] + (double)bE[j] + log((double)S2) : -INFINITY;
+            float B2 = acc[9 * tch + j], E2 = acc[10 * tch + j], S2 = acc[11 * tch + j];
+            lse_merge(B2, E2, S2, acc[12 * tch + j], acc[13 * tch + j], acc[14 * tch + j]);
+            lse_merge(B2, E2, S2, acc[15 * tch + j], acc[16 * tch + j], acc[17 * tch + j]);
+            const double v2 = (ok && S2 > 0.f) ? (double)B2 + (double)E2 + log((double)S2) : -INFINITY;
             a.part[((long long)a.nn * a.ntau + r) * a.nm_total + lo + j] = v2;
         }
     }
@@ -591,7 +628,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{24, 2}, {16, 2}, {24, 1}, {32, 2}, {32, 1}};
+static const GatherCfg kGatherCfgs[] = {{32, 1}, {24, 1}, {16, 2}, {24, 2}, {32, 2}};   // warps incl. the producer
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -606,11 +643,11 @@ template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
-    case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
-    case 2: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
-    case 3: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
-    default: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
+    case 1: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
+    case 3: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    default: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
     }
 }
 
@@ -629,7 +666,16 @@ int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 static size_t planes_smem(int tch, int dtype)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
-    return 3 * slot + 64 + (size_t)tch * 8 * 4;
+    return 3 * slot + 64 + (size_t)tch * 20 * 4;   // 6 accumulator sets of 3 floats, bcf, bsh
+}
+
+// the most templates a block can hold in shared memory next to the staged planes
+static int planes_tch_max(exm_ctx *ctx)
+{
+    const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
+    const size_t fixed = 3 * slot + 64 + 4096;   // + static shared memory (edge slots, flags)
+    const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
+    return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
 
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc)
@@ -690,7 +736,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     if (maxn <= 0) return;
     int tch = (int)((pairs + ctx->sm_count - 1) / ctx->sm_count);
     tch = std::max(tch, 256);
-    tch = std::min(((tch + 15) / 16) * 16, EXM_TCH);
+    tch = std::min(((tch + 15) / 16) * 16, planes_tch_max(ctx));
     a.tch = tch;
     a.nch = (maxn + tch - 1) / tch;
     const size_t smem = planes_smem(tch, ctx->dtype);
