@@ -202,6 +202,7 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
 #endif
 constexpr int kGroupUnroll = EXM_GUNROLL;   // tap groups of a chunk unrolled in the lane loop
 
+
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
                                            float &cS, int &fT, float &fB, float &fE, float &fS)

@@ -248,12 +248,37 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
                     rb0 = 0;
                 }
                 d.w = ((unsigned)i << 19) | ((unsigned)rd << 11) | ((unsigned)rb0 & 0x7FFu);
-                const long long ph = exm_desc_phys(pos);
-                desc[ph] = d;
-                tside[ph] = t;
+                desc[pos] = d;   // sorted order; k_tap_interleave rearranges each chunk afterwards
+                tside[pos] = t;
             }
             __syncthreads();
         }
+    }
+}
+
+// Each chunk of EXM_DCH descriptors (and time indices) of every lag, from sorted order to the
+// gather's lane-interleaved order (exm_desc_phys), in place through shared memory: writing the
+// interleaved order directly from the scatter would spread 16-byte stores over many sectors.
+__global__ void __launch_bounds__(256) k_tap_interleave(uint4 *__restrict__ desc, int32_t *__restrict__ tside,
+                                                        long long n_chunks)
+{
+    __shared__ uint4 sd[EXM_DCH];
+    __shared__ int32_t st[EXM_DCH];
+    for (long long ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+        uint4 *d = desc + ch * EXM_DCH;
+        int32_t *t = tside + ch * EXM_DCH;
+        for (int q = threadIdx.x; q < EXM_DCH; q += blockDim.x) {
+            sd[q] = d[q];
+            st[q] = t[q];
+        }
+        __syncthreads();
+        // storage index i*32 + l holds sorted position l*TPL + i
+        for (int ph = threadIdx.x; ph < EXM_DCH; ph += blockDim.x) {
+            const int q = (ph & 31) * EXM_TPL + (ph >> 5);
+            d[ph] = sd[q];
+            t[ph] = st[q];
+        }
+        __syncthreads();
     }
 }
 
@@ -332,6 +357,9 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           exm_dtype_wd(ctx->dtype), exm_dtype_calign(ctx->dtype), (int *)sl.win.p);
     k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
+    const long long n_chunks = (long long)rc * a.pitch / EXM_DCH;
+    k_tap_interleave<<<(int)std::min<long long>(n_chunks, (long long)ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+        a.desc, a.tside, n_chunks);
     EXM_CUDA(cudaGetLastError());
-    ctx->launches += 4;
+    ctx->launches += 5;
 }
