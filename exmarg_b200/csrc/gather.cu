@@ -21,6 +21,15 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+#ifndef EXM_L2HINT
+#define EXM_L2HINT 0
+#endif
+
+// the plane gather's dynamic shared memory; its parts are addressed by 32-bit byte offsets (fewer
+// registers in the tap loop than 64-bit generic pointers)
+extern __shared__ __align__(1024) unsigned char exm_gsm[];
+__device__ __forceinline__ float *gsm_f(unsigned off) { return (float *)(exm_gsm + off); }
+
 // one staged (node, lag, plane) window of element type TE: EXM_WB rows x TabElem<TE>::wd columns
 template <typename TE> __host__ __device__ constexpr int slot_elems() { return EXM_WB * TabElem<TE>::wd; }
 template <typename TE> __host__ __device__ constexpr unsigned slot_bytes() { return (unsigned)(slot_elems<TE>() * sizeof(TE)); }
@@ -62,11 +71,39 @@ __device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t 
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
+#if EXM_L2HINT
+    // the windows stream through L2 (each is staged by the few blocks of one node and lag): evicted
+    // first, so the tap descriptors that every node's block re-reads stay resident
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+        "[%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(v), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+#else
     asm volatile(
         "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
         "[%7];" ::"r"(smem_u32(dst)),
         "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(v), "r"(smem_u32(bar))
         : "memory");
+#endif
+}
+
+// a tap descriptor, kept in L2 with priority (every node's block of the lag reads it)
+__device__ __forceinline__ uint4 ld_desc(const uint4 *p)
+{
+#if EXM_L2HINT
+    uint4 v;
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+#else
+    return __ldg(p);
+#endif
 }
 
 // bounded wait on a phase of an mbarrier; false (and the error word set) if it ran out
@@ -155,40 +192,30 @@ __device__ __forceinline__ void split_double(double v, float &B, float &E)
 // Each lane takes 4 consecutive taps of a 128-tap chunk and merges equal-template taps in
 // registers; a template that lies inside one lane's taps is merged into its accumulator by
 // that lane, one that spans lanes is combined by a segmented shuffle reduction once per chunk.
+// byte offsets below are into exm_gsm
 struct RunCtx {
     const uint4 *descr;
     const int32_t *tsr;
-    const void *s0, *s1;        // the staged windows of planes p and p + 1 (element type TE)
+    unsigned s0, s1;            // the staged windows of planes p and p + 1 (element type TE)
     float sc;                   // the node's scale (16-bit tables)
-    float *aB, *aE, *aS;        // accumulators of the run's templates, index t - lo
-    const int *bsh;             // boundary runs: per-template window-row shift (index t - lo)
-    const float *bcf;           //                and beta fraction
+    unsigned acc, accst;        // accumulator set of the run's templates (B at acc + 4 (t - lo); E, S at
+                                // + accst, + 2 accst)
+    unsigned bsh, bcf;          // boundary runs: per-template window-row shift (int) and beta fraction
     const int *bnode;           // boundary runs: which templates have their boundary here
-    int lo, m_base, n, k, r, tau0, nt;
+    int lo, m_base, n, k, r;
     int sh;                     // window row of a tap = rb0 + carry + sh (regular runs)
     int up, edge;               // fast path: row <= up, and not (row == edge with beta at the clamp)
     float ckf, lw;
-    double offb_node;           // (ln s_k - beta0)/dbeta, regular runs
     int tF, tL;                 // the templates at the two ends of this warp's taps (may be shared with
-    float *eF, *eL;             // neighbouring warps): their partials go to this warp's edge slots
+    unsigned eF, eL;            // neighbouring warps): their partials go to this warp's edge slots (B, E, S)
 };
 
 __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, float E, float S)
 {
-    float *pB, *pE, *pS;
-    if (tr == c.tF) {
-        pB = c.eF;
-        pE = c.eF + 1;
-        pS = c.eF + 2;
-    } else if (tr == c.tL) {
-        pB = c.eL;
-        pE = c.eL + 1;
-        pS = c.eL + 2;
-    } else {
-        pB = c.aB + tr;
-        pE = c.aE + tr;
-        pS = c.aS + tr;
-    }
+    const bool f = tr == c.tF, l = tr == c.tL;
+    const unsigned off = f ? c.eF : (l ? c.eL : c.acc + 4u * (unsigned)tr);
+    const unsigned st = (f || l) ? 4u : c.accst;
+    float *pB = gsm_f(off), *pE = gsm_f(off + st), *pS = gsm_f(off + 2 * st);
     float b = *pB, e = *pE, s = *pS;
     lse_merge(b, e, s, B, E, S);
     *pB = b;
@@ -231,13 +258,14 @@ __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, flo
 #define EXM_SLOW_INLINE __forceinline__
 #endif
 template <bool BND, typename TE>
-__device__ EXM_SLOW_INLINE double slow_tap(const PlaneArgs &a, int il, int tm, int k, int r, int tau0, int m_base, int nt,
-                                        double offb_node, float sc)
+__device__ EXM_SLOW_INLINE double slow_tap(const PlaneArgs &a, int il, int tm, int k, int r, int m_base, float sc)
 {
+    const int nt = a.nt;
+    const int tau0 = ((a.tau[r] % nt) + nt) % nt;
     int i1 = tm + tau0;
     if (i1 >= nt) i1 -= nt;
     const int gi = il + m_base;
-    const double offb = (BND ? a.cb[gi] : offb_node) + a.boff[gi];
+    const double offb = (BND ? a.cb[gi] : a.ckd[k]) + a.boff[gi];   // ckd: (ln s_k - beta0)/dbeta
     return exm_tap_fp64<TE>(a.L[(long long)il * nt + tm], a.H[(long long)il * nt + i1], offb, r,
                             (const TE *)a.T + (long long)k * a.tstride, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
                             a.rdd, a.offd);
@@ -271,23 +299,23 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         lwv[u] = (q[u].z >> 31) ? c.lw : 0.f;
         const int rd = (int)((q[u].w >> 11) & 0xFFu);      // window column (255: outside)
         const int rb0 = ((int)(q[u].w << 21)) >> 21;        // beta-hat row from the window origin
-        const float sfr = fb + (BND ? c.bcf[ts] : c.ckf);
+        const float sfr = fb + (BND ? gsm_f(c.bcf)[ts] : c.ckf);
         const int cy = sfr >= 1.f;
         fbf[u] = cy ? sfr - 1.f : sfr;
-        const int rb = rb0 + cy + (BND ? c.bsh[ts] : c.sh);   // this node's window row
+        const int rb = rb0 + cy + (BND ? ((const int *)gsm_f(c.bsh))[ts] : c.sh);   // this node's window row
         constexpr int WD = TabElem<TE>::wd;
         fast[u] = (unsigned)rb <= (unsigned)c.up && rd <= WD - 2 && !(rb == c.edge && fbf[u] > 0.999999f);
         o[u] = fast[u] ? rb * WD + rd : 0;
     }
 #pragma unroll
     for (int u = 0; u < GRP; ++u)
-        interp_window<TE>((const TE *)c.s0, (const TE *)c.s1, o[u], fbf[u], fd[u], w[u], c.sc, vB[u], vE[u]);
+        interp_window<TE>((const TE *)(exm_gsm + c.s0), (const TE *)(exm_gsm + c.s1), o[u], fbf[u], fd[u], w[u], c.sc,
+                          vB[u], vE[u]);
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
         if (t[u] >= 0 && !fast[u]) {
             ++n_slow;
-            const double v = slow_tap<BND, TE>(a, (int)(q[u].w >> 19), c.tsr[pj + 32 * u], c.k, c.r, c.tau0, c.m_base,
-                                               c.nt, c.offb_node, c.sc);
+            const double v = slow_tap<BND, TE>(a, (int)(q[u].w >> 19), c.tsr[pj + 32 * u], c.k, c.r, c.m_base, c.sc);
             split_double(v, vB[u], vE[u]);
         }
     }
@@ -306,7 +334,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
         const int jl = jstart + TPL * lane + u;
-        qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
+        qa[u] = (jl >= beg && jl < end) ? ld_desc(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
     }
     for (int j0 = jstart; j0 < end; j0 += EXM_DCH) {
         const int jb = j0 + TPL * lane;
@@ -325,7 +353,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
 #pragma unroll
                 for (int u = 0; u < GRP; ++u) {
                     const int jl = jn0 + TPL * lane + gn + u;
-                    qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jn0 + 32 * (gn + u) + lane)
+                    qa[u] = (jl >= beg && jl < end) ? ld_desc(c.descr + jn0 + 32 * (gn + u) + lane)
                                                     : make_uint4(0u, 0u, 0u, 0u);
                 }
             }
@@ -397,7 +425,7 @@ __device__ __forceinline__ void fold_edges(float *edge, int nw, float *aB, float
 
 // this warp's equal share [w0, w1) of the run [beg, end), with its edge templates and slots
 template <bool BND, int GRP, int NW, typename TE>
-__device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, float *edge,
+__device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, unsigned edge,
                                            unsigned &n_slow)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -409,7 +437,8 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     const int q = nc / NW, rem = nc % NW;
     const int c0 = cb + warp * q + min(warp, rem), c1 = c0 + q + (warp < rem ? 1 : 0);
     const int w0 = max(beg, c0 * EXM_DCH), w1 = min(end, c1 * EXM_DCH);
-    float *e = edge + 8 * warp;
+    const unsigned eo = edge + 32u * warp;   // 8 floats per warp
+    float *e = gsm_f(eo);
     int tF = -1, tL = -1;
     if (w0 < w1) {
         tF = desc_template(c, w0);
@@ -428,8 +457,8 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     __syncwarp();
     c.tF = (tF == tL) ? -1 : tF;   // one template only: the L slot takes it all
     c.tL = tL;
-    c.eF = e;
-    c.eL = e + 4;
+    c.eF = eo;
+    c.eL = eo + 16u;
     if (w0 < w1) process_run<BND, GRP, TE>(a, c, w0, w1, n_slow);
 }
 
@@ -452,17 +481,20 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     constexpr int NC = NW - 1;   // consumer warps
     constexpr int SLOT = slot_elems<TE>();
     constexpr unsigned SLOT_B = slot_bytes<TE>();
-    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *smem = exm_gsm;
     TE *win = (TE *)smem;
     uint64_t *full = (uint64_t *)(smem + 3 * SLOT_B);   // [3] plane staged in slot s
     uint64_t *done = full + 3;                          // [2] every consumer is done with a pair (parity)
     const int tch = a.tch;
     // accumulator sets of 3 x tch floats (B, E, S): regular pairs of parity 0 / 1, regular edges
-    // (producer), boundary pairs of parity 0 / 1, boundary edges
-    float *acc = (float *)(smem + 3 * SLOT_B + 64);
+    // (producer), boundary pairs of parity 0 / 1, boundary edges; then bcf, bsh; then the edge
+    // slots [pair parity][regular, boundary][8 floats per consumer warp: F and L partials + ids]
+    const unsigned acc_o = 3 * SLOT_B + 64;
+    float *acc = gsm_f(acc_o);
     float *bcf = acc + 18 * tch;
     int *bsh = (int *)(bcf + tch);
-    __shared__ float edge[2][2][8 * NC];   // [pair parity][regular, boundary]: per warp F and L partials + ids
+    const unsigned bcf_o = acc_o + 4u * 18u * tch, bsh_o = bcf_o + 4u * tch, edge_o = bsh_o + 4u * tch;
+    auto edge_off = [&](int par, int b2) { return edge_o + 4u * (unsigned)((par * 2 + b2) * 8 * NC); };
     __shared__ int bl_sh[2];
     __shared__ unsigned bad_sh;
 
@@ -523,8 +555,9 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         for (int p = 0; p < EXM_NPAIR; ++p) {
             ok = ok && __all_sync(0xffffffffu, mbar_wait(&done[p & 1], (p >> 1) & 1, a.err));
             if (!ok) break;
-            fold_edges(edge[p & 1][0], NC, acc + 6 * tch, acc + 7 * tch, acc + 8 * tch, n);
-            if (blo < bhi) fold_edges(edge[p & 1][1], NC, acc + 15 * tch, acc + 16 * tch, acc + 17 * tch, n);
+            fold_edges(gsm_f(edge_off(p & 1, 0)), NC, acc + 6 * tch, acc + 7 * tch, acc + 8 * tch, n);
+            if (blo < bhi)
+                fold_edges(gsm_f(edge_off(p & 1, 1)), NC, acc + 15 * tch, acc + 16 * tch, acc + 17 * tch, n);
             __syncwarp();
             // plane p is no longer needed anywhere: its slot takes plane p + 3
             if (p + 3 < a.nphif) {
@@ -542,12 +575,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     } else {
         // ---------------------------------------------------------------- consumers
         const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
-        const int nt = a.nt;
         RunCtx rc;
         rc.descr = a.desc + (long long)rl * a.per_lag;
         rc.tsr = a.tside + (long long)rl * a.per_lag;
-        rc.bsh = bsh;
-        rc.bcf = bcf;
+        rc.bsh = bsh_o;
+        rc.bcf = bcf_o;
+        rc.accst = 4u * tch;
         rc.bnode = a.bnode;
         rc.lo = lo;
         rc.m_base = a.m_base;
@@ -559,10 +592,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         rc.sc = a.tsc[k];
         rc.k = k;
         rc.r = r;
-        rc.tau0 = ((a.tau[r] % nt) + nt) % nt;
-        rc.nt = nt;
         rc.lw = a.lw;
-        rc.offb_node = a.ckd[k];
         const int base_i = lo - a.m_base;   // chunk-local index of template lo
         bool ok = true;
         for (int p = 0; p < EXM_NPAIR; ++p) {
@@ -570,26 +600,20 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err));
             ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err));
             if (ok) {
-                rc.s0 = win + (p % 3) * SLOT;
-                rc.s1 = win + ((p + 1) % 3) * SLOT;
+                rc.s0 = (p % 3) * SLOT_B;
+                rc.s1 = ((p + 1) % 3) * SLOT_B;
                 const int *offp = offr + p * (a.nmc + 1) + base_i;
-                float *A = acc + 3 * (p & 1) * tch;
-                rc.aB = A;
-                rc.aE = A + tch;
-                rc.aS = A + 2 * tch;
-                warp_share<false, GRP, NC, TE>(a, rc, offp[0], offp[n], edge[p & 1][0], n_slow);
+                rc.acc = acc_o + 4u * (3u * (p & 1) * tch);
+                warp_share<false, GRP, NC, TE>(a, rc, offp[0], offp[n], edge_off(p & 1, 0), n_slow);
                 if (blo < bhi) {
-                    float *Bs = acc + (9 + 3 * (p & 1)) * tch;
-                    rc.aB = Bs;
-                    rc.aE = Bs + tch;
-                    rc.aS = Bs + 2 * tch;
+                    rc.acc = acc_o + 4u * ((9u + 3u * (p & 1)) * tch);
                     const int bb = offp[blo], be = offp[bhi];
                     n_bnd += (lane == 0 && warp == 0) ? (unsigned)(be - bb) : 0u;
-                    warp_share<true, GRP, NC, TE>(a, rc, bb, be, edge[p & 1][1], n_slow);
+                    warp_share<true, GRP, NC, TE>(a, rc, bb, be, edge_off(p & 1, 1), n_slow);
                 }
             } else if (lane == 0) {   // no work: empty edge slots for the producer
                 for (int b2 = 0; b2 < 2; ++b2) {
-                    float *e = edge[p & 1][b2] + 8 * warp;
+                    float *e = gsm_f(edge_off(p & 1, b2)) + 8 * warp;
                     e[3] = __int_as_float(-1);
                     e[7] = __int_as_float(-1);
                 }
@@ -667,14 +691,14 @@ int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 static size_t planes_smem(int tch, int dtype)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
-    return 3 * slot + 64 + (size_t)tch * 20 * 4;   // 6 accumulator sets of 3 floats, bcf, bsh
-}
+    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4;   // 6 accumulator sets of 3 floats, bcf,
+}                                                                    // bsh; edge slots
 
 // the most templates a block can hold in shared memory next to the staged planes
 static int planes_tch_max(exm_ctx *ctx)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
-    const size_t fixed = 3 * slot + 64 + 4096;   // + static shared memory (edge slots, flags)
+    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 256;   // + edge slots, static flags
     const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
     return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
