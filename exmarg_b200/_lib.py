@@ -21,7 +21,7 @@ PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 GATHER_SHAPES = ("32w x1", "24w x1", "16w x2", "24w x2", "32w x2")
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg")
@@ -50,6 +50,7 @@ def load():
         "exm_ctx_destroy": ([P], None),
         "exm_ctx_create_sharing": ([P, Z, ctypes.POINTER(P)], I),
         "exm_ctx_set_graph": ([P, I], I),
+        "exm_ctx_set_priority": ([P, I, P], I),
         "exm_last_error": ([P], ctypes.c_char_p),
         "exm_ctx_bytes": ([P], Z),
         "exm_ctx_timing": ([P, I, P], I),
@@ -131,6 +132,13 @@ class Context:
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
         self._check(self.lib.exm_ctx_set_graph(self.h, 1 if enable else 0))
+
+    def set_priority(self, priority):
+        """stream priority (0 default, lower numbers first; clamped); returns the device's
+        (greatest, least) priorities"""
+        rng = np.zeros(2, np.int32)
+        self._check(self.lib.exm_ctx_set_priority(self.h, int(priority), _p(rng)))
+        return int(rng[0]), int(rng[1])
 
     def close(self):
         if getattr(self, "h", None):

@@ -297,6 +297,26 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
     return EXM_OK;
 }
 
+extern "C" int exm_ctx_set_priority(exm_ctx *ctx, int priority, int *range_out)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    int least = 0, greatest = 0;
+    EXM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    if (range_out) {
+        range_out[0] = greatest;
+        range_out[1] = least;
+    }
+    const int prio = std::min(least, std::max(greatest, priority));
+    cudaStream_t s = nullptr;
+    EXM_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaStreamDestroy(ctx->stream);
+    ctx->stream = s;
+    if (ctx->plan) EXM_CUFFT(cufftSetStream(ctx->plan, ctx->stream));
+    API_END(ctx)
+}
+
 extern "C" int exm_ctx_set_graph(exm_ctx *ctx, int enable)
 {
     if (!ctx) return EXM_ERR_ARG;

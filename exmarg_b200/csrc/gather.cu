@@ -21,10 +21,6 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
-#ifndef EXM_L2HINT
-#define EXM_L2HINT 0
-#endif
-
 // the plane gather's dynamic shared memory; its parts are addressed by 32-bit byte offsets (fewer
 // registers in the tap loop than 64-bit generic pointers)
 extern __shared__ __align__(1024) unsigned char exm_gsm[];
@@ -71,40 +67,13 @@ __device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t 
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
-#if EXM_L2HINT
-    // the windows stream through L2 (each is staged by the few blocks of one node and lag): evicted
-    // first, so the tap descriptors that every node's block re-reads stay resident
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
-        "[%1, {%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(smem_u32(dst)),
-        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(v), "r"(smem_u32(bar)), "l"(pol)
-        : "memory");
-#else
     asm volatile(
         "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
         "[%7];" ::"r"(smem_u32(dst)),
         "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(v), "r"(smem_u32(bar))
         : "memory");
-#endif
 }
 
-// a tap descriptor, kept in L2 with priority (every node's block of the lag reads it)
-__device__ __forceinline__ uint4 ld_desc(const uint4 *p)
-{
-#if EXM_L2HINT
-    uint4 v;
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p), "l"(pol));
-    return v;
-#else
-    return __ldg(p);
-#endif
-}
 
 // bounded wait on a phase of an mbarrier; false (and the error word set) if it ran out
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err)
@@ -334,7 +303,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
         const int jl = jstart + TPL * lane + u;
-        qa[u] = (jl >= beg && jl < end) ? ld_desc(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
+        qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
     }
     for (int j0 = jstart; j0 < end; j0 += EXM_DCH) {
         const int jb = j0 + TPL * lane;
@@ -353,7 +322,7 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
 #pragma unroll
                 for (int u = 0; u < GRP; ++u) {
                     const int jl = jn0 + TPL * lane + gn + u;
-                    qa[u] = (jl >= beg && jl < end) ? ld_desc(c.descr + jn0 + 32 * (gn + u) + lane)
+                    qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jn0 + 32 * (gn + u) + lane)
                                                     : make_uint4(0u, 0u, 0u, 0u);
                 }
             }

@@ -11,7 +11,8 @@ request that has an idle worker for its bank, or whose bank can get a new worker
 HBM budget (the workspace a worker needs is first estimated from its bank's shape), up to a
 worker limit; once a worker of a bank has run, the bank's measured workspace replaces the estimate.
 Every worker uses the same gather launch shape, so a request's result does not depend
-on what else is running (bitwise).
+on what else is running (bitwise).  Requests on the device at once get stream priorities in the
+order they started, so the oldest one's gather leads and the others fill its gaps.
 """
 
 import threading
@@ -123,8 +124,19 @@ class _Worker:
         # the context may take what the device has (the scheduler keeps the sum within its budget)
         self.ctx = _lib.Context(share_store_of=parent)
         self.ctx.set_graph(graph)
+        self.priority = 0
+        self.prio_range = self.ctx.set_priority(0)     # (greatest, least)
         self.bank = bank.clone_for(self.ctx)
         prepare(self.bank, store, prior, ymin)
+
+    def prioritise(self, rank):
+        """stream priority for a request that starts while `rank` others are on the device: the
+        oldest request leads (greatest priority), later ones fill its gaps"""
+        greatest, least = self.prio_range
+        p = min(least, greatest + rank)
+        if p != self.priority:
+            self.ctx.set_priority(p)
+            self.priority = p
 
     def run(self, segments, row, seed, n_loud, n_random):
         seg = read_segments(segments, [row])       # as pe_intrinsic(rows=[row]) reads it
@@ -170,6 +182,7 @@ class Server:
             hbm_budget = int(0.85 * free)
         self.sched = Scheduler(hbm_budget, lambda k: self.cost[k], max_workers)
         self.measured = set()
+        self.running = set()            # workers with a request on the device
         self.workers = {}
         self.lock = threading.Condition()
         self.done = []
@@ -184,6 +197,10 @@ class Server:
     def _run(self, req, wid):
         try:
             w = self.workers[wid]
+            with self.lock:
+                rank = len(self.running)
+                self.running.add(wid)
+            w.prioritise(rank)
             req.t_start = time.perf_counter()
             lnl, lnb = w.run(req.segments, req.row, req.seed, self.n_loud, self.n_random)
             req.t_done = time.perf_counter()
@@ -194,6 +211,7 @@ class Server:
             used = None
             req.future.set_exception(e)
         with self.lock:
+            self.running.discard(wid)
             if used is not None and req.key not in self.measured:   # the estimate gives way to the measured size
                 self.measured.add(req.key)
                 self.sched.recost(req.key, used, self.cost.__setitem__)

@@ -68,6 +68,14 @@ EXM_API int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ctx *
  * selection, taps, gather, epilogue -- as one CUDA graph, captured on the first segment
  * of a shape and replayed for the rest.  No reference counterpart. */
 EXM_API int exm_ctx_set_graph(exm_ctx *ctx, int enable);
+
+/* Scheduling priority of the context's stream (CUDA stream priorities: 0 is the default and
+ * lower numbers run first; clamped to the device's range, which *range_out receives as
+ * {greatest, least} if not NULL).  Contexts analysing segments at the same time compete for
+ * the SMs block by block; a server that gives its workers distinct priorities lets one
+ * segment's gather lead while the others fill its gaps, instead of interleaving all of them
+ * (which multiplies the tap descriptors resident in L2).  No reference counterpart. */
+EXM_API int exm_ctx_set_priority(exm_ctx *ctx, int priority, int *range_out);
 EXM_API const char *exm_last_error(const exm_ctx *ctx);
 /* Bytes of device memory the context holds now. */
 EXM_API size_t exm_ctx_bytes(const exm_ctx *ctx);
