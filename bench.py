@@ -403,6 +403,8 @@ def run_b200(args):
                     "latency_ms_p50": 1000.0 * float(np.percentile(lat, 50)),
                     "latency_ms_p99": 1000.0 * float(np.percentile(lat, 99))},
             "gpu_launches": int(tm["launches"]),
+            "exact_path_taps_per_step": tm["slow_taps"] / args.steps,
+            "boundary_taps_per_step": tm["boundary_taps"] / args.steps,
             "stages_ms_per_step": {k: tm[k] / args.steps for k in ("filter_ms", "select_ms", "taps_ms", "gather_ms",
                                                                     "epilogue_ms")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

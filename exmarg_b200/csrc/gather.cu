@@ -203,22 +203,19 @@ constexpr int kGroupUnroll = EXM_GUNROLL;   // tap groups of a chunk unrolled in
 __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
                                            float &cS, int &fT, float &fB, float &fE, float &fS)
 {
-    if (t != cT) {
-        if (cT >= 0) {   // cT closes here: the lane's first closed partial, or one inside the lane
-            if (fT < 0) {
-                fT = cT;
-                fB = cB;
-                fE = cE;
-                fS = cS;
-            } else {
-                acc_merge(c, cT, cB, cE, cS);
-            }
-        }
-        cT = t;          // an empty partial: the merge below makes it (vB, vE, vS)
-        cB = -1e30f;
-        cE = 0.f;
-        cS = 0.f;
-    }
+    // branch-free except for the rare template that opens and closes inside one lane
+    const bool nw = t != cT;
+    const bool close = nw && cT >= 0;      // cT closes here
+    const bool toF = close && fT < 0;      // ... as the lane's first closed partial
+    if (close && !toF) acc_merge(c, cT, cB, cE, cS);
+    fT = toF ? cT : fT;
+    fB = toF ? cB : fB;
+    fE = toF ? cE : fE;
+    fS = toF ? cS : fS;
+    cT = nw ? t : cT;                      // a new template starts from an empty partial
+    cB = nw ? -1e30f : cB;
+    cE = nw ? 0.f : cE;
+    cS = nw ? 0.f : cS;
     lse_merge(cB, cE, cS, vB, vE, t >= 0 ? 1.f : 0.f);
 }
 
