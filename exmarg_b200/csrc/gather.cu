@@ -177,6 +177,7 @@ struct RunCtx {
     float ckf, lw;
     int tF, tL;                 // the templates at the two ends of this warp's taps (may be shared with
     unsigned eF, eL;            // neighbouring warps): their partials go to this warp's edge slots (B, E, S)
+    unsigned q, qn;             // this warp's queue of exact-path taps for the pair (int2 entries) and its count
 };
 
 __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, float E, float S)
@@ -197,11 +198,12 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
 #define EXM_GUNROLL 2
 #endif
 constexpr int kGroupUnroll = EXM_GUNROLL;   // tap groups of a chunk unrolled in the lane loop
+#define EXM_SLOWQ 8   // exact-path taps a consumer warp queues per plane pair for the producer
 
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
-__device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, int &cT, float &cB, float &cE,
-                                           float &cS, int &fT, float &fB, float &fE, float &fS)
+__device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, float vE, float wt, int &cT, float &cB,
+                                           float &cE, float &cS, int &fT, float &fB, float &fE, float &fS)
 {
     // branch-free except for the rare template that opens and closes inside one lane
     const bool nw = t != cT;
@@ -216,7 +218,7 @@ __device__ __forceinline__ void lane_merge(const RunCtx &c, int t, float vB, flo
     cB = nw ? -1e30f : cB;
     cE = nw ? 0.f : cE;
     cS = nw ? 0.f : cS;
-    lse_merge(cB, cE, cS, vB, vE, t >= 0 ? 1.f : 0.f);
+    lse_merge(cB, cE, cS, vB, vE, wt);
 }
 
 // the exact float64 value of a tap outside the staged window (rare)
@@ -277,16 +279,42 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
     for (int u = 0; u < GRP; ++u)
         interp_window<TE>((const TE *)(exm_gsm + c.s0), (const TE *)(exm_gsm + c.s1), o[u], fbf[u], fd[u], w[u], c.sc,
                           vB[u], vE[u]);
+    float wt[GRP];
 #pragma unroll
     for (int u = 0; u < GRP; ++u) {
-        if (t[u] >= 0 && !fast[u]) {
-            ++n_slow;
-            const double v = slow_tap<BND, TE>(a, (int)(q[u].w >> 19), c.tsr[pj + 32 * u], c.k, c.r, c.m_base, c.sc);
-            split_double(v, vB[u], vE[u]);
+        const bool sl = t[u] >= 0 && !fast[u];
+        wt[u] = t[u] >= 0 ? 1.f : 0.f;
+        if (__any_sync(0xffffffffu, sl)) {
+            // exact-path taps go to the warp's queue: the producer computes them 32 at a time instead
+            // of stalling the warp on one lane's float64 path; a full queue computes them here
+            const int lane = threadIdx.x & 31;
+            const unsigned m = __ballot_sync(0xffffffffu, sl);
+            int *qn = (int *)(exm_gsm + c.qn);
+            const int n0 = *qn;
+            const int pos = n0 + __popc(m & ((1u << lane) - 1u));
+            __syncwarp();
+            if (sl) {
+                ++n_slow;
+                if (pos < EXM_SLOWQ) {
+                    ((int2 *)(exm_gsm + c.q))[pos] =
+                        make_int2(pj + 32 * u, (int)(q[u].w >> 19) | (BND ? 1 << 30 : 0) | (int)((q[u].z >> 31) << 29));
+                    vB[u] = -1e30f;
+                    vE[u] = 0.f;
+                    wt[u] = 0.f;
+                    lwv[u] = 0.f;
+                } else {
+                    const double v =
+                        slow_tap<BND, TE>(a, (int)(q[u].w >> 19), c.tsr[pj + 32 * u], c.k, c.r, c.m_base, c.sc);
+                    split_double(v, vB[u], vE[u]);
+                }
+            }
+            if (lane == 0) *qn = min(EXM_SLOWQ, n0 + __popc(m));
+            __syncwarp();
         }
     }
 #pragma unroll
-    for (int u = 0; u < GRP; ++u) lane_merge(c, t[u], vB[u], vE[u] + lwv[u], cT, cB, cE, cS, fT, fB, fE, fS);
+    for (int u = 0; u < GRP; ++u)
+        lane_merge(c, t[u], vB[u], vE[u] + lwv[u], wt[u], cT, cB, cE, cS, fT, fB, fE, fS);
 }
 
 template <bool BND, int GRP, typename TE>
@@ -460,6 +488,11 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     float *bcf = acc + 18 * tch;
     int *bsh = (int *)(bcf + tch);
     const unsigned bcf_o = acc_o + 4u * 18u * tch, bsh_o = bcf_o + 4u * tch, edge_o = bsh_o + 4u * tch;
+    // exact-path queues [pair mod 3][consumer warp]: counts, then EXM_SLOWQ int2 entries (storage index of the
+    // tap; template | boundary flag << 30 | random-draw flag << 29)
+    const unsigned qcnt_o = edge_o + 4u * (2 * 2 * 8 * 32), qent_o = qcnt_o + 4u * 3 * 32;
+    int *qcnt = (int *)(smem + qcnt_o);
+    const int2 *qent = (const int2 *)(smem + qent_o);
     auto edge_off = [&](int par, int b2) { return edge_o + 4u * (unsigned)((par * 2 + b2) * 8 * NC); };
     __shared__ int bl_sh[2];
     __shared__ unsigned bad_sh;
@@ -512,6 +545,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 
     if (warp == NC) {
         // ---------------------------------------------------------------- producer
+        const int32_t *tsr_all = a.tside + (long long)rl * a.per_lag;
         int issued = 0;
         if (lane == 0)
             for (int q = 0; q < 3 && q < a.nphif; ++q)
@@ -529,6 +563,58 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             if (p + 3 < a.nphif) {
                 if (lane == 0) tma_load_plane(&tmap, &full[p % 3], win + (p % 3) * SLOT, C0, R0, p + 3, r, k, SLOT_B);
                 ++issued;
+            }
+            // the exact-path taps the consumers queued for pair p: 32 lanes compute them, lane 0 merges them
+            // in warp and queue order into the producer's sets (the consumers reuse these queues at pair
+            // p + 3, after plane p + 4, which is staged only after this)
+            {
+                const int par = p % 3;
+                const int cw = lane < NC ? qcnt[par * 32 + lane] : 0;
+                int incl = cw;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                const int excl = incl - cw;
+                for (int b0 = 0; b0 < total; b0 += 32) {
+                    const int i = b0 + lane;
+                    double v = 0.0;
+                    int tr = 0, bnd = 0;
+                    int wi = 0;   // the warp whose entries [excl, incl) hold i (shuffles kept converged)
+                    for (int l = 1; l < NC; ++l) {
+                        const int el = __shfl_sync(0xffffffffu, excl, l);
+                        wi += (i < total && el <= i) ? 1 : 0;
+                    }
+                    const int wexcl = __shfl_sync(0xffffffffu, excl, wi);
+                    if (i < total) {
+                        const int2 e = qent[(par * 32 + wi) * EXM_SLOWQ + (i - wexcl)];
+                        const int il = e.y & 0x1FFF;
+                        bnd = (e.y >> 30) & 1;
+                        const int tm = tsr_all[e.x];
+                        v = bnd ? slow_tap<true, TE>(a, il, tm, k, r, a.m_base, a.tsc[k])
+                                : slow_tap<false, TE>(a, il, tm, k, r, a.m_base, a.tsc[k]);
+                        v += ((e.y >> 29) & 1) ? (double)a.lw : 0.0;
+                        tr = il + a.m_base - lo;
+                    }
+                    const int nb2 = min(32, total - b0);
+                    for (int qq = 0; qq < nb2; ++qq) {
+                        const double vq = __shfl_sync(0xffffffffu, v, qq);
+                        const int tq = __shfl_sync(0xffffffffu, tr, qq), bq = __shfl_sync(0xffffffffu, bnd, qq);
+                        if (lane == 0 && tq >= 0 && tq < n) {
+                            float B, E;
+                            split_double(vq, B, E);
+                            float *F = acc + (bq ? 15 : 6) * tch;
+                            float b = F[tq], x = F[tch + tq], sv = F[2 * tch + tq];
+                            lse_merge(b, x, sv, B, E, 1.f);
+                            F[tq] = b;
+                            F[tch + tq] = x;
+                            F[2 * tch + tq] = sv;
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
         if (!ok) {
@@ -565,6 +651,10 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             // warp-uniform: the lanes go on to shuffles together
             ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err));
             ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err));
+            if (lane == 0) qcnt[(p % 3) * 32 + warp] = 0;
+            __syncwarp();
+            rc.qn = qcnt_o + 4u * ((p % 3) * 32 + warp);
+            rc.q = qent_o + 8u * (((p % 3) * 32 + warp) * EXM_SLOWQ);
             if (ok) {
                 rc.s0 = (p % 3) * SLOT_B;
                 rc.s1 = ((p + 1) % 3) * SLOT_B;
@@ -619,7 +709,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{32, 1}, {24, 1}, {16, 2}, {24, 2}, {32, 2}};   // warps incl. the producer
+static const GatherCfg kGatherCfgs[] = {{16, 2}, {24, 2}, {24, 1}, {32, 1}, {32, 2}};   // warps incl. the producer
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -634,10 +724,10 @@ template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
-    case 1: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
-    case 2: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
-    case 3: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
+    case 1: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
+    case 3: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
     default: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
     }
 }
@@ -657,14 +747,15 @@ int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 static size_t planes_smem(int tch, int dtype)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
-    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4;   // 6 accumulator sets of 3 floats, bcf,
-}                                                                    // bsh; edge slots
+    // 6 accumulator sets of 3 floats, bcf, bsh; edge slots; exact-path queue counts and entries
+    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8;
+}
 
 // the most templates a block can hold in shared memory next to the staged planes
 static int planes_tch_max(exm_ctx *ctx)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
-    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 256;   // + edge slots, static flags
+    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 256;
     const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
     return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
