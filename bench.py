@@ -285,27 +285,33 @@ def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, 
 
 
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
-    """the same segments served by exmarg_b200.serve.Server: child contexts sharing the resident
-    tables, two banks (all 2048 templates and the first 1024), graph replay on the workers.
-    'batched': every request queued at once (segments in flight together); 'poisson': arrivals at
-    80 % of the plain path's capacity.  Served ln Lambda of the 2048-template bank is compared
-    bitwise with the plain call's."""
+    """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
+    banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
+    segments (n_time 16384) -- in equal parts, graph replay on the workers.  'batched': every request
+    queued at once (segments in flight together); 'poisson': arrivals at 80 % of the plain path's
+    2048-template 8 s capacity.  Served ln Lambda of the 2048-template 8 s bank is compared bitwise
+    with the plain call's."""
     import exmarg_b200 as eb
+    from exmarg_b200 import synth
     from exmarg_b200.serve import Request, Server, latency_stats
     half = eb.MassBank(rows[:1024, 0], rows[:1024, 1], rows[:1024, 2], seg, "b200", device_index=local)
-    banks = {"bank2048": bank, "bank1024": half}
+    seg4 = synth.make_segments(8, segment_seed(0) + 777, T=4.0, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
+    short = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg4, "b200", device_index=local)
+    banks = {"bank2048": bank, "bank1024": half, "bank2048_4s": short}
+    segs = {"bank2048": seg, "bank1024": seg, "bank2048_4s": seg4}
     first = args.warmup
     n_req = args.serve_requests
     n_rows = len(plain)
-    mix = [("bank2048" if i % 3 else "bank1024", first + (i % n_rows)) for i in range(n_req)]
+    keys = ("bank2048", "bank1024", "bank2048_4s")
+    mix = [(keys[i % 3], first + (i % n_rows) if i % 3 < 2 else i % 8) for i in range(n_req)]
     out = {}
     srv = Server(store, banks, device=local, max_workers=args.serve_workers, graph=True)
     try:
         # warm-up with the same mix (workers per bank as the mix needs them: allocation, FFT plans,
         # graph capture happen here)
-        srv.serve([Request(-1 - i, k, seg, row=0) for i, (k, _) in enumerate(mix[:4 * args.serve_workers])])
+        srv.serve([Request(-1 - i, k, segs[k], row=0) for i, (k, _) in enumerate(mix[:4 * args.serve_workers])])
         for leg in ("batched", "poisson"):
-            reqs = [Request(i, k, seg, row=r) for i, (k, r) in enumerate(mix)]
+            reqs = [Request(i, k, segs[k], row=r) for i, (k, r) in enumerate(mix)]
             if leg == "batched":
                 arrivals = None
             else:
@@ -320,7 +326,8 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
             st = latency_stats(done)
             d = {"requests": n_req, "workers": args.serve_workers, "segments_per_s": st["segments_per_s"],
                  "latency_ms_p50": st["p50_ms"], "latency_ms_p99": st["p99_ms"],
-                 "identical_to_plain": same, "banks": "2048 and 1024 templates (2:1)"}
+                 "identical_to_plain": same,
+                 "banks": "2048 templates / 8 s, 1024 / 8 s, 2048 / 4 s segments (1:1:1)"}
             if leg == "poisson":
                 d["offered_per_s"] = 0.8 * capacity
             out[leg] = d

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import exmarg_b200 as eb
-from exmarg_b200 import MassBank, _lib
+from exmarg_b200 import MassBank, _lib, synth
 from exmarg_b200.serve import Request, Server, latency_stats
 from exmarg_b200.store import upload_store
 from tests.golden_io import Fixture
@@ -48,14 +48,21 @@ def _mix(fx, keys, n):
 @pytest.mark.parametrize("budget", ["ample", "one_worker"])
 def test_served_results_equal_plain(budget):
     fx = Fixture("config1")
-    banks = {"all": fx.b200_bank(), "odd": _sub_bank(fx, np.arange(1, 64, 2)), "low": _sub_bank(fx, np.arange(20))}
+    # a bank on segments of half the duration (half n_time) beside the fixture's: same store and lags
+    short_seg = synth.make_segments(2, 321, T=fx.seg["T"] / 2, fmin=fx.seg["fmin"], fmax=fx.seg["fmax"], snr=12.0)
+    short = MassBank(fx.rows[:, 0], fx.rows[:, 1], fx.rows[:, 2], short_seg, "b200")
+    banks = {"all": fx.b200_bank(), "odd": _sub_bank(fx, np.arange(1, 64, 2)), "low": _sub_bank(fx, np.arange(20)),
+             "short": short}
+    segs = {k: fx.seg for k in banks}
+    segs["short"] = short_seg
     expect = {}
     for k, b in banks.items():
-        r = _pe(fx, b)
-        for row in range(fx.seg["d_H"].shape[0]):
+        r = eb.pe_intrinsic(segs[k], b, fx.store, prior=fx.prior_arg, ymin=fx.ymin, n_loud=fx.n_loud,
+                            n_random=fx.n_random, seed=0)
+        for row in range(segs[k]["d_H"].shape[0]):
             expect[(k, row)] = (r["ln_lambda"][row], float(r["ln_b"][row]))
-    mix = _mix(fx, sorted(banks), 14)
-    reqs = [Request(i, k, fx.seg, row=row, seed=0) for i, (k, row) in enumerate(mix)]
+    mix = _mix(fx, sorted(banks), 16)
+    reqs = [Request(i, k, segs[k], row=row, seed=0) for i, (k, row) in enumerate(mix)]
     srv = Server(fx.store, banks, max_workers=3, prior=fx.prior_arg, ymin=fx.ymin, n_loud=fx.n_loud,
                  n_random=fx.n_random)
     if budget == "one_worker":     # one worker at a time: banks take turns, idle ones are evicted
