@@ -369,7 +369,7 @@ def run_b200(args):
         tune = {"chosen": args.gather_cfg, "forced": True}
     elif not args.no_tune:
         best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
-        tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:5]],
+        tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:len(_lib.GATHER_SHAPES)]],
                 "shapes": list(_lib.GATHER_SHAPES)}
     ctx.timing(True)
     if pg:

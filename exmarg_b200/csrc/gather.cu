@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{16, 2}, {24, 2}, {24, 1}, {32, 1}, {32, 2}};   // warps incl. the producer
+static const GatherCfg kGatherCfgs[] = {{20, 2}, {16, 2}, {24, 2}, {24, 1}, {32, 1}, {32, 2}};   // warps incl. producer
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -724,10 +724,11 @@ template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
-    case 1: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
-    case 2: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
-    case 3: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<20, 2, TE>(ctx, a, grid, smem); break;
+    case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    case 3: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
+    case 4: launch_planes<32, 1, TE>(ctx, a, grid, smem); break;
     default: launch_planes<32, 2, TE>(ctx, a, grid, smem); break;
     }
 }

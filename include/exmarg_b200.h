@@ -158,7 +158,9 @@ EXM_API int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const d
  * group): replays the gather of the last segment analysed by exm_pe_intrinsic on this
  * context (same n_loud, n_random) once per shape, times each with CUDA events (reps
  * launches), keeps the fastest for later calls and writes its index to best_cfg and the
- * ms per launch of every shape to ms_per_cfg (if not NULL; exm_gather_num_cfgs entries).
+ * ms per launch of every shape to ms_per_cfg (if not NULL; room for 16 entries: this build
+ * has 6 shapes, warps per block including the producer warp x taps per register group:
+ * 20x2, 16x2, 24x2, 24x1, 32x1, 32x2).
  * No reference counterpart (the reference takes block as a kwarg, pe.py:289-290). */
 EXM_API int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, double *ms_per_cfg);
 
