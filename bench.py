@@ -252,7 +252,7 @@ def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, 
             st = synth.MemoryStore(spec, s_nodes, TABLE_SEED, tables=[None] * len(s_nodes), table_dtype=dt)
             st.generator = (M, P, Q, S, TABLE_SEED)
             eb.prepare(b, st, "volume", 0.1267)
-            ctx.set_gather_cfg(gather_cfg)
+            ctx.set_gather_cfg(*gather_cfg)
         d = {}
         try:
             if dt != "f32":
@@ -369,7 +369,10 @@ def run_b200(args):
         tune = {"chosen": args.gather_cfg, "forced": True}
     elif not args.no_tune:
         best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
-        tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:len(_lib.GATHER_SHAPES)]],
+        ns = len(_lib.GATHER_SHAPES)
+        tune = {"chosen": int(best), "ms_per_shape": [round(float(x), 3) for x in ms[:ns]],
+                "chunk_pct_chosen": ctx.gather_chunk_pct,
+                "ms_per_chunk_pct": {str(p): round(float(x), 3) for p, x in zip((50, 150, 200), ms[ns:ns + 3])},
                 "shapes": list(_lib.GATHER_SHAPES)}
     ctx.timing(True)
     if pg:
@@ -439,7 +442,7 @@ def run_b200(args):
         line["parity"] = {"templates": n_t, "max_abs_dlnlambda": float(np.abs(lnl_gpu - lnl_cpu).max()),
                           "sample_dlnB": float(abs(restate.log_mean(lnl_gpu, cell) - restate.log_mean(lnl_cpu, cell)))}
         if args.prec_templates > 0:
-            cfg = ctx.gather_cfg if ctx.gather_cfg is not None else 0
+            cfg = (ctx.gather_cfg if ctx.gather_cfg is not None else 0, ctx.gather_chunk_pct)
             line["precision"] = precision_legs(args, spec, s_nodes, rows, bank, store, store_h, cfg, local)
         del store_h
     if rank == 0:

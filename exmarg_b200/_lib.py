@@ -68,8 +68,8 @@ def load():
         "exm_gather": ([P, I, I, P, P, P, P], I),
         "exm_node_values": ([P, P], I),
         "exm_gather_noalloc": ([P, I, I, P, P, P, P, I, P, P, I, I, P, P, P, P], I),
-        "exm_autotune": ([P, I, I, I, P, P], I),
-        "exm_set_gather_cfg": ([P, I], I),
+        "exm_autotune": ([P, I, I, I, P, P, P], I),
+        "exm_set_gather_cfg": ([P, I, I], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -128,6 +128,7 @@ class Context:
         self.prep_token = None
         self.nm = self.nfreq = self.n_time = None
         self.gather_cfg = None          # the launch shape chosen by autotune or set_gather_cfg (None: default)
+        self.gather_chunk_pct = 100     # templates per gather block, percent of the default
 
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
@@ -273,15 +274,21 @@ class Context:
     def autotune(self, n_loud=1024, n_random=1024, reps=2):
         """time every launch shape of the plane gather on the last segment; keep the fastest.
         returns (best index, ms per launch of each shape)"""
-        best = ctypes.c_int()
+        best, pct = ctypes.c_int(), ctypes.c_int()
         ms = np.zeros(16, np.float64)
-        self._check(self.lib.exm_autotune(self.h, int(n_loud), int(n_random), int(reps), ctypes.byref(best), _p(ms)))
+        self._check(self.lib.exm_autotune(self.h, int(n_loud), int(n_random), int(reps), ctypes.byref(best),
+                                          ctypes.byref(pct), _p(ms)))
         self.gather_cfg = best.value
+        self.gather_chunk_pct = pct.value
         return best.value, ms
 
-    def set_gather_cfg(self, cfg):
-        self._check(self.lib.exm_set_gather_cfg(self.h, int(cfg)))
+    def set_gather_cfg(self, cfg, chunk_pct=0):
+        """launch shape (index into GATHER_SHAPES) and templates per block in percent of the default
+        (0 keeps the current)"""
+        self._check(self.lib.exm_set_gather_cfg(self.h, int(cfg), int(chunk_pct)))
         self.gather_cfg = int(cfg)
+        if chunk_pct:
+            self.gather_chunk_pct = int(chunk_pct)
 
     def node_values(self, n_nodes):
         out = np.empty((n_nodes + 1, self.nm), np.float64)

@@ -282,6 +282,7 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         ctx->tmap = parent->tmap;
         ctx->tmap_ok = parent->tmap_ok;
         ctx->gather_cfg = parent->gather_cfg;
+        ctx->gather_chunk_pct = parent->gather_chunk_pct;
         exm_ensure(ctx, ctx->d_stats, 4 * sizeof(unsigned long long));
         EXM_CUDA(cudaMemset(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long)));
     } catch (const exm_error &e) {
@@ -954,7 +955,8 @@ extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, cons
 
 // ------------------------------------------------------------------ autotuner
 
-extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, double *ms_per_cfg)
+extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, int *best_chunk_pct,
+                            double *ms_per_cfg)
 {
     API_BEGIN(ctx)
     EXM_CUDA(cudaSetDevice(ctx->dev));
@@ -972,10 +974,7 @@ extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, in
     const int keep = ctx->gather_cfg;
     const bool tim = ctx->tim_on;
     ctx->tim_on = false;
-    double best = 1e300;
-    int arg = keep;
-    for (int c = 0; c < n; ++c) {
-        ctx->gather_cfg = c;
+    auto time_gather = [&]() {
         exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);   // warm-up (and function attributes)
         EXM_CUDA(cudaEventRecord(e0, ctx->stream));
         for (int r = 0; r < std::max(1, reps); ++r) exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);
@@ -983,27 +982,53 @@ extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, in
         EXM_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         EXM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        const double per = ms / std::max(1, reps);
+        return ms / std::max(1, reps);
+    };
+    // 1: every launch shape with the default template chunk
+    double best = 1e300;
+    int arg = keep;
+    ctx->gather_chunk_pct = 100;
+    for (int c = 0; c < n; ++c) {
+        ctx->gather_cfg = c;
+        const double per = time_gather();
         if (ms_per_cfg) ms_per_cfg[c] = per;
         if (per < best) {
             best = per;
             arg = c;
         }
     }
+    // 2: the templates per gather block (percent of the one-wave-per-lag size) with the best shape
+    static const int pcts[] = {50, 150, 200};
+    int best_pct = 100;
+    ctx->gather_cfg = arg;
+    for (int i = 0; i < 3; ++i) {
+        ctx->gather_chunk_pct = pcts[i];
+        const double per = time_gather();
+        if (ms_per_cfg) ms_per_cfg[n + i] = per;
+        if (per < best) {
+            best = per;
+            best_pct = pcts[i];
+        }
+    }
+    ctx->gather_chunk_pct = best_pct;
     ctx->tim_on = tim;
     ctx->gather_cfg = arg;
     if (best_cfg) *best_cfg = arg;
+    if (best_chunk_pct) *best_chunk_pct = best_pct;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     check_dev_err(ctx, sl);
     API_END(ctx)
 }
 
-extern "C" int exm_set_gather_cfg(exm_ctx *ctx, int cfg)
+extern "C" int exm_set_gather_cfg(exm_ctx *ctx, int cfg, int chunk_pct)
 {
     API_BEGIN(ctx)
     REQUIRE(cfg >= 0 && cfg < exm_gather_num_cfgs(), EXM_ERR_ARG, "no such gather launch shape");
+    REQUIRE(chunk_pct == 0 || (chunk_pct >= 10 && chunk_pct <= 1000), EXM_ERR_ARG,
+            "chunk_pct must be 0 (keep) or 10..1000");
     ctx->gather_cfg = cfg;
+    if (chunk_pct) ctx->gather_chunk_pct = chunk_pct;
     API_END(ctx)
 }
 

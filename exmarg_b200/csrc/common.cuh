@@ -126,6 +126,7 @@ struct exm_ctx {
 
     // launch shape of the plane gather (index into its table; chosen by exm_autotune)
     int gather_cfg = 0;
+    int gather_chunk_pct = 100;   // templates per gather block, percent of the one-wave-per-lag size
 
     // cuFFT
     cufftHandle plan = 0;

@@ -756,7 +756,7 @@ static size_t planes_smem(int tch, int dtype)
 static int planes_tch_max(exm_ctx *ctx)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
-    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 256;
+    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 2048;   // + static
     const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
     return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
@@ -818,6 +818,7 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     }
     if (maxn <= 0) return;
     int tch = (int)((pairs + ctx->sm_count - 1) / ctx->sm_count);
+    tch = (int)((long long)tch * ctx->gather_chunk_pct / 100);
     tch = std::max(tch, 256);
     tch = std::min(((tch + 15) / 16) * 16, planes_tch_max(ctx));
     a.tch = tch;
