@@ -365,8 +365,8 @@ def run_b200(args):
         eb.pe_intrinsic(seg, bank, store, rows=[i])
     tune = None
     if args.gather_cfg >= 0:
-        ctx.set_gather_cfg(args.gather_cfg)
-        tune = {"chosen": args.gather_cfg, "forced": True}
+        ctx.set_gather_cfg(args.gather_cfg, args.gather_chunk_pct)
+        tune = {"chosen": args.gather_cfg, "chunk_pct": ctx.gather_chunk_pct, "forced": True}
     elif not args.no_tune:
         best, ms = ctx.autotune(N_LOUD, N_RANDOM, reps=2)
         ns = len(_lib.GATHER_SHAPES)
@@ -466,6 +466,8 @@ def main():
     ap.add_argument("--nodes", type=int, default=53, help="store nodes (reduced profiling cases)")
     ap.add_argument("--lags", type=int, default=87, help="table lags (reduced profiling cases; odd)")
     ap.add_argument("--gather-cfg", type=int, default=-1, help="force a gather launch shape (no autotuning)")
+    ap.add_argument("--gather-chunk-pct", type=int, default=0,
+                    help="with --gather-cfg: templates per gather block in percent of the default (0: 100)")
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")

@@ -64,9 +64,10 @@ def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, 
 
 
 def autotune(bank, store, segments, prior="volume", ymin=0.1267, n_loud=1024, n_random=1024, reps=2):
-    """choose the plane gather's launch shape for this bank and store: analyse the first segment
-    once, then time every shape on it (CUDA events); later calls on the context use the fastest.
-    returns (chosen shape index, ms per launch of each shape)"""
+    """choose the plane gather's launch shape and templates per block for this bank and store: analyse
+    the first segment once, then time every shape on it (CUDA events), then the block size at 50 / 150 /
+    200% with the best shape; later calls on the context use the fastest.
+    returns (chosen shape index, ms per launch: each shape, then each block size)"""
     pe_intrinsic(segments, bank, store, rows=[0], prior=prior, ymin=ymin, n_loud=n_loud, n_random=n_random)
     return bank.ctx.autotune(n_loud, n_random, reps)
 
