@@ -284,6 +284,31 @@ def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, 
     return out
 
 
+def batched_leg(args, store, bank, local):
+    """the batched workload: n segments with network SNR drawn from U(0, 30), 30 % noise-only, float32
+    strain, analysed by one pe_intrinsic call on a context that replays each segment as a captured CUDA
+    graph (the 2048-template bank and resident store of the main run)"""
+    import exmarg_b200 as eb
+    from exmarg_b200 import synth
+    n = args.batch_segments
+    segs = synth.make_segments(n + 1, segment_seed(0) + 4242, T=T_SEG, fmax=FMAX, snr=(0.0, 30.0), noise_only=0.3,
+                               mc=(10.0, 40.0), q=(0.25, 1.0), chi=(-0.5, 0.5), dtype=np.complex64)
+    ctx = bank.ctx
+    ctx.set_graph(True)
+    try:
+        eb.pe_intrinsic(segs, bank, store, rows=[0])          # first segment of the shape: runs, then is captured
+        ctx.timing(True)
+        t0 = time.perf_counter()
+        res = eb.pe_intrinsic(segs, bank, store, rows=list(range(1, n + 1)))
+        wall = time.perf_counter() - t0
+        tm = ctx.timing(False)
+    finally:
+        ctx.set_graph(False)
+    return {"segments": n, "segments_per_s": n / (tm["total_ms"] / 1000.0), "e2e_segments_per_s": n / wall,
+            "snr": "U(0, 30), 30% noise-only", "strain": "complex64", "graph_replay": True,
+            "ln_b_range": [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]}
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
@@ -425,6 +450,8 @@ def run_b200(args):
             "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
+    if rank == 0 and world == 1 and args.batch_segments > 0:
+        line["batched"] = batched_leg(args, store, bank, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -471,6 +498,7 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--batch-segments", type=int, default=16, help="segments of the batched leg (0: none)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
     ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
     args = ap.parse_args()
