@@ -351,6 +351,8 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
             st = latency_stats(done)
             d = {"requests": n_req, "workers": args.serve_workers, "segments_per_s": st["segments_per_s"],
                  "latency_ms_p50": st["p50_ms"], "latency_ms_p99": st["p99_ms"],
+                 "service_ms_p50": st["service_ms_p50"], "service_ms_max": st["service_ms_max"],
+                 "workers_created": srv.n_created, "workers_evicted": srv.n_evicted,
                  "identical_to_plain": same,
                  "banks": "2048 templates / 8 s, 1024 / 8 s, 2048 / 4 s segments (1:1:1)"}
             if leg == "poisson":

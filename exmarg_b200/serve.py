@@ -45,9 +45,10 @@ def workspace_bytes(nm, n_time, n_nodes, n_lags, nfreq, nwalk):
 class Scheduler:
     """admission by workspace budget; no device work (the server drives it)
 
-    workers: key -> list of worker ids; a new worker for key costs cost(key) bytes.  When a queued
-    request needs budget or a worker slot, idle workers of banks with no queued requests are evicted.
-    A request whose bank has workers, all busy, waits for one of them when nothing can be evicted."""
+    workers: key -> list of worker ids; a new worker for key costs cost(key) bytes.  A request whose
+    bank has no worker may evict idle workers of banks with no queued requests to get budget or a
+    worker slot; a request whose bank has workers, all busy, gets another only from free budget and
+    slots, else it waits for one of them."""
 
     def __init__(self, budget, cost, max_workers):
         self.budget, self.cost, self.max_workers = int(budget), cost, int(max_workers)
@@ -64,13 +65,16 @@ class Scheduler:
         self.queue.append((item, key))
 
     def _take_worker(self, key):
-        for w in self.workers.get(key, []):
+        mine = self.workers.get(key, [])
+        for w in mine:
             if w not in self.busy:
                 return w, False, []
         c = self.cost(key)
         evicted = []
-        # make room by closing idle workers of other banks (never a busy one)
-        while self.used + c > self.budget or self.n_workers() >= self.max_workers:
+        # make room by closing idle workers of other banks (never a busy one) -- only for a bank that has
+        # no worker at all: a bank whose workers are busy waits for one, since opening a worker (context,
+        # workspace, FFT plans, graph capture) costs more than a segment
+        while mine == [] and (self.used + c > self.budget or self.n_workers() >= self.max_workers):
             w = self._evict_one(key)
             if w is None:
                 break
@@ -182,6 +186,7 @@ class Server:
             hbm_budget = int(0.85 * free)
         self.sched = Scheduler(hbm_budget, lambda k: self.cost[k], max_workers)
         self.measured = set()
+        self.n_created = self.n_evicted = 0   # workers opened and closed for budget (diagnostics)
         self.running = set()            # workers with a request on the device
         self.workers = {}
         self.lock = threading.Condition()
@@ -191,6 +196,7 @@ class Server:
 
     def _worker_for(self, wid, key):
         if wid not in self.workers:
+            self.n_created += 1
             self.workers[wid] = _Worker(self.parent, self.banks[key], self.store, self.prior, self.ymin, self.graph)
         return self.workers[wid]
 
@@ -229,6 +235,7 @@ class Server:
                 w = self.workers.pop(e, None)
                 if w is not None:
                     w.close()
+                    self.n_evicted += 1
             if req is None:
                 return n
             if new:
@@ -274,8 +281,14 @@ class Server:
 
 
 def latency_stats(requests):
-    lat = np.array([r.t_done - r.t_arrival for r in requests if r.t_done is not None])
+    """arrival-to-result latency percentiles, throughput over the served window, and the service time
+    (start to result) apart from the queueing"""
+    done = [r for r in requests if r.t_done is not None]
+    lat = np.array([r.t_done - r.t_arrival for r in done])
+    svc = np.array([r.t_done - r.t_start for r in done if r.t_start is not None])
     t0 = min(r.t_arrival for r in requests)
-    t1 = max(r.t_done for r in requests)
+    t1 = max(r.t_done for r in done)
     return {"requests": len(lat), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "p99_ms": float(np.percentile(lat, 99) * 1e3), "segments_per_s": len(lat) / (t1 - t0)}
+            "p99_ms": float(np.percentile(lat, 99) * 1e3), "segments_per_s": len(lat) / (t1 - t0),
+            "service_ms_p50": float(np.percentile(svc, 50) * 1e3) if svc.size else None,
+            "service_ms_max": float(svc.max() * 1e3) if svc.size else None}

@@ -86,3 +86,18 @@ def test_idle_worker_with_queued_work_is_kept():
     g = s.admit()
     assert g[0] == "a1" and g[2] == a[2] and g[4] == []
     assert s.admit()[0] is None                         # b0 waits for the budget
+
+
+def test_busy_bank_waits_instead_of_evicting():
+    cost = {"a": 40, "b": 40}
+    s = Scheduler(budget=100, cost=lambda k: cost[k], max_workers=2)
+    s.push("a0", "a")
+    s.push("b0", "b")
+    a = s.admit()
+    b = s.admit()
+    s.release(b[2])                                     # 'b' idle, 'a' busy
+    s.push("a1", "a")
+    g = s.admit()
+    assert g[0] is None and g[4] == []                  # no second 'a' worker at the price of 'b''s
+    s.release(a[2])
+    assert s.admit()[0] == "a1"
