@@ -24,7 +24,8 @@ GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2")
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
-           "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg")
+           "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
+           "exm_redshift_grid", "exm_source_frame")
 
 _lib = None
 
@@ -70,6 +71,8 @@ def load():
         "exm_gather_noalloc": ([P, I, I, P, P, P, P, I, P, P, I, I, P, P, P, P], I),
         "exm_autotune": ([P, I, I, I, P, P, P], I),
         "exm_set_gather_cfg": ([P, I, I], I),
+        "exm_redshift_grid": ([P, I, I, P, P, I, P, P, I, P, P], I),
+        "exm_source_frame": ([P, P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -239,12 +242,13 @@ class Context:
         out = np.ascontiguousarray(np.stack([traj["lqH"], traj["phH"], traj["lqL"], traj["phL"]]), np.float32)
         self._check(self.lib.exm_set_trajectories(self.h, _p(out)))
 
-    def select_times(self, seed, n_loud, n_random):
+    def select_times(self, seed, n_loud, n_random, want=True):
+        """the visited times (on the device); with want, also (sel, lw) on the host"""
         nw = n_loud + n_random
-        sel = np.empty((self.nm, nw), np.int32)
-        lw = np.empty((self.nm, nw), np.float32)
+        sel = np.empty((self.nm, nw), np.int32) if want else None
+        lw = np.empty((self.nm, nw), np.float32) if want else None
         self._check(self.lib.exm_select_times(self.h, int(seed), int(n_loud), int(n_random), _p(sel), _p(lw)))
-        return sel, lw
+        return (sel, lw) if want else None
 
     def set_times(self, times):
         if times is None:
@@ -289,6 +293,21 @@ class Context:
         self.gather_cfg = int(cfg)
         if chunk_pct:
             self.gather_chunk_pct = int(chunk_pct)
+
+    def redshift_grid(self, yN, Mdet, yq, z, m1, w):
+        """pe_redshift's grid on the device (exm_redshift_grid)"""
+        yN, Mdet, yq, z, m1, w = (np.ascontiguousarray(x, np.float64) for x in (yN, Mdet, yq, z, m1, w))
+        self._check(self.lib.exm_redshift_grid(self.h, yN.shape[0], yN.shape[1], _p(yN), _p(Mdet), z.size, _p(yq),
+                                               _p(z), m1.size, _p(m1), _p(w)))
+        self.rs_shape = (m1.size, z.size)
+
+    def source_frame(self, lamN, want=True):
+        """(ln_lambda (nm1, nz) or None, ln_b) of one segment's node values"""
+        lamN = np.ascontiguousarray(lamN, np.float64)
+        out = np.empty(self.rs_shape, np.float64) if want else None
+        lnb = np.zeros(1, np.float64)
+        self._check(self.lib.exm_source_frame(self.h, _p(lamN), _p(out), _p(lnb)))
+        return out, float(lnb[0])
 
     def node_values(self, n_nodes):
         out = np.empty((n_nodes + 1, self.nm), np.float64)

@@ -329,6 +329,7 @@ static void ctx_free(exm_ctx *ctx)
 {
     cudaSetDevice(ctx->dev);
     cudaStreamSynchronize(ctx->stream);
+    exm_redshift_release(ctx);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->plan) cufftDestroy(ctx->plan);
     if (ctx->store_borrowed) {   // the parent owns the tables

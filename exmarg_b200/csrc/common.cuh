@@ -125,6 +125,7 @@ struct exm_ctx {
     dbuf d_stats;                     // uint64 [4]: gather counters (slow-path taps, boundary taps)
 
     // launch shape of the plane gather (index into its table; chosen by exm_autotune)
+    struct exm_redshift *rs = nullptr;   // pe_redshift's grid and buffers (csrc/redshift.cu)
     int gather_cfg = 0;
     int gather_chunk_pct = 100;   // templates per gather block, percent of the one-wave-per-lag size
 

@@ -154,6 +154,7 @@ __device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, 
 // ------------------------------------------------------------------ launchers
 
 void exm_store_quantize(exm_ctx *ctx, int k, const float *src, int sp);
+void exm_redshift_release(exm_ctx *ctx);
 void exm_store_dequantize(exm_ctx *ctx, int k, float *dst, int dp);
 
 void exm_fft_plan(exm_ctx *ctx, int batch);

@@ -94,3 +94,85 @@ def distance_weights(y, prior, ymin):
             w[i + 1] += np.trapezoid(f * (t - a) / h, t)
     with np.errstate(divide="ignore"):
         return np.log(w)
+
+
+# ----------------------------------------------------------------------------- pe_redshift
+
+_DL_CACHE = {}
+
+
+def _dl_grid(zmax, nz):
+    key = (float(zmax), int(nz))
+    if key not in _DL_CACHE:
+        from .cosmology import dl_of_z
+        z = np.linspace(0.02, zmax, int(nz))
+        _DL_CACHE[key] = (z, dl_of_z(z))
+    return _DL_CACHE[key]
+
+
+def _node_y(store, u, ymin):
+    """y = sqrt(a), a = s/u, of each (node, template) pair the store covers, and row n_node the boundary
+    point (exmarg/search/pe.py:58-84; 0 where a template has no point)"""
+    s = np.asarray(store.s, float)
+    nn = s.size
+    y = np.zeros((nn + 1, u.size))
+    for k in range(nn):
+        alo = min(store.alpha_lo[k], ymin * ymin)
+        a = s[k] / u
+        o = (np.sqrt(a) >= ymin) & (a > alo) & (a < store.alpha_hi[k])
+        y[k] = np.where(o, np.sqrt(a), 0.0)
+        s_prev = s[k - 1] if k > 0 else 0.0
+        low = o & (s_prev / u <= alo)
+        y[nn][low] = np.sqrt(float(alo) * (1.0 + 1e-9))
+    return y
+
+
+def pe_redshift(segments, bank, store, rows=None, chunk=8, zmax=8.0, nz=1600, m1_range=(3.0, 150.0), nm1=1600,
+                ymin=0.1267, nodes_per_launch=6, block=256, mdet_range=(10.0, 500.0), resident=False, n_loud=1024,
+                n_random=1024, seed=0):
+    """ln Lambda(m1_source, z) of each segment (the contract of exmarg/search/pe.py:203-257).
+
+    bank: an ascending equal-mass, zero-spin bank of detector-frame total masses.  With a 'b200' bank
+    every segment runs filter, time selection and the plane gather on the device (exm_filter,
+    exm_select_times, exm_node_values), then the source frame and ln B (exm_source_frame); chunk,
+    nodes_per_launch, block and resident are accepted and have no effect.  D_L(z) is
+    exmarg_b200.cosmology's restatement of Planck 2018 (the reference uses astropy's Planck18).
+
+    returns dict: m1 (nm1,), z (nz,), ln_lambda (n_segment, nm1, nz), ln_b (n_segment,), rows."""
+    if getattr(bank, "device", None) in ("cpu", "gpu"):
+        import exmarg.search as ref
+        return ref.pe_redshift(segments, bank, store, rows=rows, chunk=chunk, zmax=zmax, nz=nz, m1_range=m1_range,
+                               nm1=nm1, ymin=ymin, nodes_per_launch=nodes_per_launch, block=block,
+                               mdet_range=mdet_range, resident=resident, n_loud=n_loud, n_random=n_random, seed=seed)
+    if getattr(bank, "device", None) != "b200":
+        raise ValueError("device must be 'cpu', 'gpu' or 'b200'")
+    M = np.asarray(bank.M, float)
+    if np.any(np.diff(M) <= 0) or np.any(np.asarray(bank.q) != 1.0) or np.any(np.asarray(bank.chi) != 0.0):
+        raise ValueError("pe_redshift needs an ascending equal-mass zero-spin bank")
+    from .segments import D0
+    seg = read_segments(segments, rows)
+    z, dl = _dl_grid(zmax, nz)
+    m1 = np.geomspace(m1_range[0], m1_range[1], int(nm1))
+    ctx = prepare(bank, store, "volume", ymin)
+    key = (ctx.bank_token, ctx.store_token, float(ymin), float(zmax), int(nz), float(m1_range[0]),
+           float(m1_range[1]), int(nm1), float(mdet_range[0]), float(mdet_range[1]))
+    if getattr(ctx, "rs_key", None) != key:
+        lnp = np.log(np.maximum((1.0 + z) * dl ** 2 * np.gradient(dl, z), 1e-300))
+        Md = 2.0 * m1[:, None] * (1.0 + z[None, :])
+        inside = (Md >= mdet_range[0]) & (Md <= mdet_range[1])
+        w = np.where(inside, np.exp(lnp)[None, :], 0.0) * np.gradient(m1)[:, None] * np.gradient(z)[None, :]
+        w /= w.sum()
+        ctx.redshift_grid(_node_y(store, np.asarray(bank.u, float), ymin), M, D0 / dl, z, m1, w)
+        ctx.rs_key = key
+    nn = len(store.s)
+    out = np.full((seg["rows"].size, m1.size, z.size), -np.inf)
+    ln_b = np.empty(seg["rows"].size)
+    for e, row in enumerate(seg["rows"]):
+        ctx.filter(seg["d_H"][e:e + 1], seg["d_L"][e:e + 1], seg["sig2_H"], seg["sig2_L"], want=False)
+        if n_loud > 0:
+            ctx.select_times(seed + int(row), n_loud, n_random, want=False)
+        else:
+            ctx.set_times(None)
+        lamN = ctx.node_values(nn)
+        out[e], ln_b[e] = ctx.source_frame(lamN)
+    return dict(m1=m1, z=z, ln_lambda=out, ln_b=ln_b, rows=seg["rows"])

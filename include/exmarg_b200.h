@@ -220,6 +220,20 @@ EXM_API int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float *lq
                                int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,
                                double *out);
 
+/* pe_redshift's grid (exmarg/search/pe.py:203-257): the node geometry's y values yN
+ * (nn1 = n_nodes + 1 rows, row n_nodes the boundary point, nm templates in bank order), the
+ * bank's detector-frame total masses Mdet (ascending), the z grid and yq = D0 / D_L(z) (nz),
+ * the source-frame primary masses m1 (nm1) and the normalised prior weights w (nm1, nz).
+ * Kept on the device for exm_source_frame; replaces a previous grid.  No counterpart in the
+ * reference as a separate call (it is part of its pe_redshift). */
+EXM_API int exm_redshift_grid(exm_ctx *ctx, int nn1, int nm, const double *yN, const double *Mdet, int nz,
+                      const double *yq, const double *z, int nm1, const double *m1, const double *w);
+
+/* One segment's source frame (exmarg/search/pe.py:87-132, _to_source_frame, and the ln B of
+ * :249-255): node values lamN (nn1, nm, as exm_node_values gives them) -> ln_lambda_out
+ * (nm1, nz; may be NULL) and ln_b_out, float64, on the grid of exm_redshift_grid. */
+EXM_API int exm_source_frame(exm_ctx *ctx, const double *lamN, double *ln_lambda_out, double *ln_b_out);
+
 /* Node values of the current segment (exmarg/search/pe.py:168-200,
  * _node_values): lamN_out (n_nodes + 1, nm) float64, -inf where a template does
  * not reach a node; row n_nodes the boundary point.  Uses the plane-staged gather. */

@@ -335,3 +335,88 @@ def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0
     if return_parts:
         res["parts"] = parts
     return res
+
+
+# ----------------------------------------------------------------------------- pe_redshift
+
+def source_frame(lamN, yN, Mdet, yq, m1, z):
+    """exmarg/search/pe.py:87-132 (_to_source_frame, numpy): node values (n_node + 1, n_template) ->
+    ln Lambda (nm1, nz): linear in y per template between its finite node values, then linear in
+    M_det = 2 m1 (1 + z) per z between the finite templates"""
+    L, Y = np.asarray(lamN, float), np.asarray(yN, float)
+    ok = np.isfinite(L) & (Y > 0)
+    Yk = np.where(ok, Y, np.inf)
+    order = np.argsort(Yk, axis=0, kind="stable")
+    Ys = np.take_along_axis(Yk, order, axis=0)
+    Ls = np.take_along_axis(L, order, axis=0)
+    n = ok.sum(axis=0)
+    nm = Ys.shape[1]
+    cols = np.arange(nm)[None, :]
+    j = (Ys[:, None, :] <= np.asarray(yq)[None, :, None]).sum(axis=0) - 1
+    lo = np.clip(j, 0, np.maximum(n - 2, 0)[None, :])
+    hi = np.minimum(lo + 1, np.maximum(n - 1, 0)[None, :])
+    y0, y1, v0, v1 = Ys[lo, cols], Ys[hi, cols], Ls[lo, cols], Ls[hi, cols]
+    yq_ = np.asarray(yq)[:, None]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t = np.where(y1 > y0, (yq_ - y0) / np.where(y1 > y0, y1 - y0, 1.0), 1.0)
+        ylast = Ys[np.maximum(n - 1, 0), np.arange(nm)][None, :]
+        inside = (n[None, :] >= 2) & (yq_ >= Ys[0][None, :]) & (yq_ <= ylast)
+        surf = np.where(inside, v0 + t * (v1 - v0), -np.inf)
+    M = np.asarray(Mdet, float)
+    good = np.isfinite(surf)
+    rank = np.cumsum(good, axis=1)
+    ngood = rank[:, -1]
+    G = np.zeros(surf.shape, np.int64)
+    iz, im = np.nonzero(good)
+    G[iz, rank[iz, im] - 1] = im
+    Md = 2.0 * np.asarray(m1)[:, None] * (1.0 + np.asarray(z))[None, :]
+    p = np.searchsorted(M, Md.ravel()).reshape(Md.shape)
+    zi = np.arange(len(z))[None, :]
+    below = np.where(p > 0, rank[zi, np.maximum(p - 1, 0)], 0)
+    lo = G[zi, np.clip(below - 1, 0, None)]
+    hi = G[zi, np.minimum(below, np.maximum(ngood - 1, 0)[None, :])]
+    lo = np.where(below >= 1, lo, hi)
+    m0, m1_ = M[lo], M[hi]
+    w0, w1 = surf[zi, lo], surf[zi, hi]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        t = np.where(m1_ > m0, (Md - m0) / np.where(m1_ > m0, m1_ - m0, 1.0), 0.0)
+        first = M[G[:, 0]][None, :]
+        last = M[G[zi[0], np.maximum(ngood - 1, 0)]][None, :]
+        inb = (ngood[None, :] >= 2) & (Md >= first) & (Md <= last)
+        return np.where(inb, w0 + t * (w1 - w0), -np.inf)
+
+
+def redshift_weights(m1, z, dl, mdet_range):
+    """exmarg/search/pe.py:249-254: prior weights on the (m1, z) cells, uniform in M_det on mdet_range
+    and proportional to (1 + z) D_L^2 dD_L/dz; normalised"""
+    lnp = np.log(np.maximum((1.0 + z) * dl ** 2 * np.gradient(dl, z), 1e-300))
+    Md = 2.0 * m1[:, None] * (1.0 + z[None, :])
+    inside = (Md >= mdet_range[0]) & (Md <= mdet_range[1])
+    w = np.where(inside, np.exp(lnp)[None, :], 0.0) * np.gradient(m1)[:, None] * np.gradient(z)[None, :]
+    return w / w.sum()
+
+
+def pe_redshift(seg, W, u, M, lo, n_time, store, dl_of_z, zmax=8.0, nz=1600, m1_range=(3.0, 150.0), nm1=1600,
+                ymin=0.1267, nodes_per_launch=6, mdet_range=(10.0, 500.0), n_loud=1024, n_random=1024, seed=0,
+                precision="ref"):
+    """exmarg/search/pe.py:203-257 for the segments of seg (read_segments output): ln Lambda (n_seg, nm1, nz)
+    on z = linspace(0.02, zmax, nz), m1 = geomspace(*m1_range, nm1), and ln B; dl_of_z is the distance
+    function (the reference's is astropy's Planck18)"""
+    from exmarg_b200.segments import D0
+    z = np.linspace(0.02, zmax, int(nz))
+    m1 = np.geomspace(m1_range[0], m1_range[1], int(nm1))
+    dl = dl_of_z(z)
+    yq = D0 / dl
+    geometry = node_geometry(store.s, store.alpha_lo, store.alpha_hi, u, ymin)
+    nn = store.s.size
+    groups = [list(range(g, min(g + nodes_per_launch, nn))) for g in range(0, nn, nodes_per_launch)]
+    out = np.full((seg["rows"].size, m1.size, z.size), -np.inf)
+    for e in range(seg["rows"].size):
+        traj = trajectories(W, {I: seg["d_" + I][e] for I in "HL"}, {I: seg["sig2_" + I] for I in "HL"}, lo,
+                            n_time, precision)
+        tm = select_times(traj, store.tau_idx, n_loud, n_random, seed + int(seg["rows"][e])) if n_loud > 0 else None
+        lamN = node_values(traj, store, geometry, groups, tm)
+        out[e] = source_frame(lamN, geometry[2], M, yq, m1, z)
+    w = redshift_weights(m1, z, dl, mdet_range)
+    ln_b = np.array([log_mean(L, w) for L in out])
+    return dict(m1=m1, z=z, ln_lambda=out, ln_b=ln_b)

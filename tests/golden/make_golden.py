@@ -1,7 +1,7 @@
 """Golden vectors for the pe_intrinsic path, produced by running the REFERENCE's own CPU
 code (exmarg.search: numpy + numba) in a container where its source tree is present.
 
-    python tests/golden/make_golden.py [reference src dir]
+    python tests/golden/make_golden.py [reference src dir [case ...]]
 
 Each fixture holds the inputs (segments, bank rows, W and u, the store geometry and the
 float32 generator factors of its seeded tables) and the reference's outputs (ln_lambda,
@@ -83,11 +83,72 @@ def make(name, c, search):
     print(name, "ln_b", res["ln_b"], "size %.1f MB" % (os.path.getsize(os.path.join(HERE, "%s.npz" % name)) / 1e6))
 
 
+# pe_redshift: an ascending equal-mass, zero-spin bank of detector-frame total masses, 8 s segments, a
+# reduced (m1, z) grid.  The reference takes D_L from astropy's Planck18, absent here: a stand-in module
+# hands it exmarg_b200.cosmology.dl_of_z (the same restatement the B200 path uses), so these vectors pin
+# everything but the distance function itself.
+REDSHIFT_CASES = {
+    "redshift1": dict(T=8.0, fmax=256.0, ntau=43, nb=100, nd=109, nodes=(10, 14, 18, 22, 26, 30, 34),
+                      masses=(12.0, 200.0, 24), n_seg=2, snr=(10.0, 25.0), n_loud=512, n_random=512, seed_seg=1300,
+                      seed_tab=29, zmax=4.0, nz=160, m1_range=(3.0, 100.0), nm1=140),
+}
+
+
+def stub_astropy():
+    import types
+    from exmarg_b200 import cosmology
+
+    class _Quantity:
+        def __init__(self, v):
+            self.value = v
+
+    class _Planck18:
+        @staticmethod
+        def luminosity_distance(z):
+            return _Quantity(cosmology.dl_of_z(z))
+
+    mod = types.ModuleType("astropy")
+    cos = types.ModuleType("astropy.cosmology")
+    cos.Planck18 = _Planck18
+    mod.cosmology = cos
+    sys.modules["astropy"] = mod
+    sys.modules["astropy.cosmology"] = cos
+
+
+def make_redshift(name, c, search):
+    stub_astropy()
+    spec = synth.TableSpec(ntau=c["ntau"], nphif=49, nb=c["nb"], nd=c["nd"])
+    s_nodes = synth.S_NODES_PROD[list(c["nodes"])]
+    store = synth.MemoryStore(spec, s_nodes, c["seed_tab"])
+    seg = synth.make_segments(c["n_seg"], c["seed_seg"], T=c["T"], fmax=c["fmax"], snr=c["snr"])
+    lo_m, hi_m, n_m = c["masses"]
+    M = np.geomspace(lo_m, hi_m, n_m)
+    rows = np.stack([M, np.ones_like(M), np.zeros_like(M)], axis=1)
+    bank = search.mass_bank(rows, seg, "cpu")
+    res = search.pe_redshift(seg, bank, store, zmax=c["zmax"], nz=c["nz"], m1_range=c["m1_range"], nm1=c["nm1"],
+                             n_loud=c["n_loud"], n_random=c["n_random"], seed=0)
+    M_, P, Q, S = spec.factors(s_nodes)
+    out = dict(d_H=seg["d_H"], d_L=seg["d_L"], f=seg["f"], nu=seg["nu"], sig2=seg["sig2"], T=seg["T"],
+               fmin=seg["fmin"], fmax=seg["fmax"], bank_rows=rows, W=bank.W, u=bank.u, lo=bank.lo,
+               n_time=bank.n_time, s_nodes=s_nodes, tab_seed=c["seed_tab"], ntau=spec.ntau, nb=spec.nb, nd=spec.nd,
+               ymin=0.1267, n_loud=c["n_loud"], n_random=c["n_random"], zmax=c["zmax"], nz=c["nz"],
+               m1_lo=c["m1_range"][0], m1_hi=c["m1_range"][1], nm1=c["nm1"], m1=res["m1"], z=res["z"],
+               ln_lambda=res["ln_lambda"], ln_b=res["ln_b"], fac_M=M_, fac_P=P, fac_Q=Q, fac_S=S, prior="volume")
+    np.savez_compressed(os.path.join(HERE, "%s.npz" % name), **out)
+    print(name, "ln_b", res["ln_b"], "finite", np.isfinite(res["ln_lambda"]).mean(),
+          "size %.1f MB" % (os.path.getsize(os.path.join(HERE, "%s.npz" % name)) / 1e6))
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
     search = refimport.import_reference(src)
+    only = sys.argv[2:] if len(sys.argv) > 2 else None
     for name, c in CASES.items():
-        make(name, c, search)
+        if only is None or name in only:
+            make(name, c, search)
+    for name, c in REDSHIFT_CASES.items():
+        if only is None or name in only:
+            make_redshift(name, c, search)
 
 
 if __name__ == "__main__":
