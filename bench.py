@@ -309,6 +309,26 @@ def batched_leg(args, store, bank, local):
             "ln_b_range": [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]}
 
 
+def redshift_leg(args, store, seg, local):
+    """pe_redshift as the reference's published timing runs it: a 120-template equal-mass, zero-spin bank of
+    detector-frame total masses, 8 s segments on the resident 53-node store, the default (m1, z) grid of
+    1600 x 1600, n_loud = n_random = 1024; ln Lambda on the grid is copied back for every segment.  Total
+    masses run 8..150 Msun: above that the inspiral's ISCO frequency (4400 Hz Msun / M) falls below the 20 Hz
+    band edge and a template has no power"""
+    import exmarg_b200 as eb
+    M = np.geomspace(8.0, 150.0, 120)
+    bank = eb.MassBank(M, np.ones_like(M), np.zeros_like(M), seg, "b200", device_index=local)
+    n = min(args.redshift_segments, seg["d_H"].shape[0] - 1)
+    eb.pe_redshift(seg, bank, store, rows=[0])          # grid set-up and first-call costs
+    t0 = time.perf_counter()
+    res = eb.pe_redshift(seg, bank, store, rows=list(range(1, n + 1)))
+    wall = time.perf_counter() - t0
+    return {"segments": n, "templates": 120, "grid": "1600 m1 x 1600 z", "s_per_segment": wall / n,
+            "segments_per_s": n / wall, "reference_published_s_per_segment": 0.102,
+            "reference_published_hardware": "1 L40S, cupy, batches of 16",
+            "ln_b_range": [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]}
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
@@ -454,6 +474,8 @@ def run_b200(args):
         line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
     if rank == 0 and world == 1 and args.batch_segments > 0:
         line["batched"] = batched_leg(args, store, bank, local)
+    if rank == 0 and world == 1 and args.redshift_segments > 0:
+        line["redshift"] = redshift_leg(args, store, seg, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -500,6 +522,7 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--redshift-segments", type=int, default=8, help="segments of the pe_redshift leg (0: none)")
     ap.add_argument("--batch-segments", type=int, default=16, help="segments of the batched leg (0: none)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
     ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
