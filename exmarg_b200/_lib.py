@@ -25,7 +25,11 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame")
+           "exm_redshift_grid", "exm_source_frame", "exm_store_load")
+
+LOAD_DIRECT = 1
+LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
+              "issue_wait_seconds")
 
 _lib = None
 
@@ -73,6 +77,7 @@ def load():
         "exm_set_gather_cfg": ([P, I, I], I),
         "exm_redshift_grid": ([P, I, I, P, P, I, P, P, I, P, P], I),
         "exm_source_frame": ([P, P, P, P], I),
+        "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -183,6 +188,32 @@ class Context:
     def store_set_node(self, k, s, alpha_lo, alpha_hi, T):
         T = np.ascontiguousarray(T, np.float32)
         self._check(self.lib.exm_store_set_node(self.h, k, s, alpha_lo, alpha_hi, _p(T)))
+
+    def store_load(self, first, s, alpha_lo, alpha_hi, paths=None, offsets=None, hosts=None, readers=6, chunk_bytes=0,
+                   direct=False):
+        """nodes first.. from files (paths[i] at byte offsets[i]) or host tables (hosts[i], where paths[i] is
+        None) in one pipelined pass; returns the loader's statistics (LOAD_STATS)"""
+        n = len(s)
+        s, alo, ahi = (np.ascontiguousarray(x, np.float64) for x in (s, alpha_lo, alpha_hi))
+        if not (alo.size == ahi.size == n):
+            raise ValueError("one s, alpha_lo, alpha_hi per node")
+        c_paths = c_offs = c_hosts = None
+        keep = []
+        if paths is not None:
+            if len(paths) != n or offsets is None or len(offsets) != n:
+                raise ValueError("one path and one offset per node")
+            c_paths = (ctypes.c_char_p * n)(*[None if p is None else os.fsencode(p) for p in paths])
+            c_offs = np.ascontiguousarray([0 if o is None else int(o) for o in offsets], np.int64)
+        if hosts is not None:
+            if len(hosts) != n:
+                raise ValueError("one host table (or None) per node")
+            keep = [None if h is None else np.ascontiguousarray(h, np.float32) for h in hosts]
+            c_hosts = (ctypes.c_void_p * n)(*[None if h is None else h.ctypes.data for h in keep])
+        st = np.zeros(len(LOAD_STATS))
+        self._check(self.lib.exm_store_load(self.h, int(first), n, c_paths, _p(c_offs), c_hosts, _p(s), _p(alo), _p(ahi),
+                                            int(readers), int(chunk_bytes), LOAD_DIRECT if direct else 0, _p(st)))
+        del keep
+        return dict(zip(LOAD_STATS, st.tolist()))
 
     def store_generate_node(self, k, s, alpha_lo, alpha_hi, M, P, Q, S, seed):
         M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))

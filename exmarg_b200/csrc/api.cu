@@ -496,6 +496,33 @@ extern "C" int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo
     API_END(ctx)
 }
 
+extern "C" int exm_store_load(exm_ctx *ctx, int first, int n, const char *const *paths, const int64_t *offsets,
+                              const float *const *hosts, const double *s, const double *alpha_lo, const double *alpha_hi,
+                              int readers, long long chunk_bytes, int flags, double *stats_out)
+{
+    API_BEGIN(ctx)
+    REQUIRE(!ctx->store_borrowed, EXM_ERR_STATE, "this context borrows its parent's store");
+    REQUIRE(ctx->n_children.load() == 0, EXM_ERR_STATE, "child contexts borrow this store: destroy them first");
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(ctx->T.p, EXM_ERR_STATE, "exm_store_init first");
+    REQUIRE(n >= 1 && first >= 0 && first + n <= ctx->nn, EXM_ERR_ARG, "node range outside the store");
+    REQUIRE(s && alpha_lo && alpha_hi, EXM_ERR_ARG, "null node metadata");
+    REQUIRE(paths || hosts, EXM_ERR_ARG, "neither files nor host tables");
+    REQUIRE(!paths || offsets, EXM_ERR_ARG, "files without offsets");
+    REQUIRE(readers >= 1 && readers <= 64, EXM_ERR_ARG, "readers must be 1..64");
+    REQUIRE(chunk_bytes >= 0, EXM_ERR_ARG, "negative chunk size");
+    REQUIRE((flags & ~EXM_LOAD_DIRECT) == 0, EXM_ERR_ARG, "unknown load flags");
+    for (int i = 0; i < n; ++i) {
+        REQUIRE(s[i] > 0 && alpha_lo[i] > 0 && alpha_hi[i] > alpha_lo[i], EXM_ERR_ARG,
+                "node needs s > 0 and 0 < alpha_lo < alpha_hi");
+        REQUIRE(i == 0 || s[i] > s[i - 1], EXM_ERR_ARG, "nodes must be added with s ascending");
+    }
+    if (first > 0 && ctx->node_set[first - 1]) REQUIRE(s[0] > ctx->s[first - 1], EXM_ERR_ARG, "nodes must be added with s ascending");
+    exm_store_load_run(ctx, first, n, paths, offsets, hosts, readers, chunk_bytes, flags, stats_out);
+    for (int i = 0; i < n; ++i) set_node_meta(ctx, first + i, s[i], alpha_lo[i], alpha_hi[i]);
+    API_END(ctx)
+}
+
 extern "C" int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *M,
                                        const float *P, const float *Q, float S, uint32_t seed)
 {

@@ -154,6 +154,9 @@ __device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, 
 // ------------------------------------------------------------------ launchers
 
 void exm_store_quantize(exm_ctx *ctx, int k, const float *src, int sp);
+// nodes first..first+n-1 from files (at byte offsets) or host arrays through pinned staging (storeio.cu)
+void exm_store_load_run(exm_ctx *ctx, int first, int n, const char *const *paths, const int64_t *offsets,
+                        const float *const *hosts, int readers, long long chunk_bytes, int flags, double *stats);
 void exm_redshift_release(exm_ctx *ctx);
 void exm_store_dequantize(exm_ctx *ctx, int k, float *dst, int dp);
 

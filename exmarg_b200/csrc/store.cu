@@ -4,7 +4,7 @@
 // per-node scale (value = scale * element): float16 uses the power of two that puts
 // the node's largest |value| just below 2^15 (so scaling is exact and the range
 // fits), bfloat16 has float32's range and a scale of 1.  Both round to nearest even.
-// Replaces exmarg/search/store.py:204-214 (upload): the tables are copied once and
+// Replaces exmarg/search/store.py:110-120 (upload): the tables are copied once and
 // stay resident for every call.
 #include <cudaTypedefs.h>
 

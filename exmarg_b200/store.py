@@ -5,6 +5,10 @@ beta, Delta) float32, beta, delta, tau_idx, alpha, s_node), sorted by s_node, in
 host memory (or maps them with mmap=True), exactly like the reference.  For
 device='b200' the tables are copied once into HBM by the analysis context and
 stay resident for every later call (upload_store); there is no per-call upload.
+That copy is one pipelined pass of the native loader (exm_store_load): reader
+threads fill pinned buffers while earlier chunks go to the device.  A store
+loaded with mmap=True is streamed straight from its files (nothing is read into
+host memory first), optionally with O_DIRECT (direct=True).
 """
 
 import glob
@@ -63,14 +67,28 @@ class RedshiftStore:
     n_max: int
     device_tokens: dict = field(default_factory=dict, repr=False)
     table_dtype: str = "f32"
+    files: list = None          # the bd_*.npz of each node
+    t_offsets: list = None      # byte offset of each node's T.npy data (None: not float32 C-order)
+    mapped: bool = False        # tables are maps of the files (mmap=True)
+    readers: int = 6
+    direct: bool = False
+    load_stats: dict = field(default=None, repr=False)
 
 
 TABLE_DTYPES = {"f32": _lib.DTYPE_F32, "f16": _lib.DTYPE_F16, "bf16": _lib.DTYPE_BF16}
 
 
-def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dtype="f32"):
+def _table_offset(path):
+    """byte offset of the T.npy data in a bd_*.npz when it is float32 in C order (else None)"""
+    off, shape, fortran, dtype = _member_offset(path, "T.npy")
+    return off if (np.dtype(dtype) == np.dtype("<f4") and (not fortran or len(shape) <= 1)) else None
+
+
+def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dtype="f32", direct=False):
     """every node of the store in host memory (about 0.75 GB per node at the production shape);
-    pinned is accepted for the reference's signature (the b200 path copies each table to HBM once).
+    pinned is accepted for the reference's signature (the b200 upload stages through its own pinned
+    buffers).  mmap=True maps the tables instead; the b200 upload then streams them from the files
+    with `readers` threads, with O_DIRECT when direct=True.
     table_dtype: how the b200 path keeps the tables in HBM -- 'f32' (as stored), or 'f16' / 'bf16'
     (half the bytes; see quantize_table for the values it then uses)"""
     if table_dtype not in TABLE_DTYPES:
@@ -92,7 +110,9 @@ def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dt
             tables = list(ex.map(lambda f: read_npz_member(f, "T.npy"), files))
     return RedshiftStore(s=np.array(s), alpha_lo=np.array(alo), alpha_hi=np.array(ahi), beta=list(beta),
                          delta=list(delta), tau_idx=tau[0], tables=tables,
-                         n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]), table_dtype=table_dtype)
+                         n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]), table_dtype=table_dtype,
+                         files=list(files), t_offsets=[_table_offset(f) for f in files], mapped=bool(mmap),
+                         readers=max(1, min(64, int(readers))), direct=bool(direct))
 
 
 def with_table_dtype(store, table_dtype):
@@ -160,13 +180,24 @@ def upload_store(store, ctx):
     beta0, dbeta, delta0, ddelta = store_grid(store)
     dtype = TABLE_DTYPES[getattr(store, "table_dtype", "f32")]
     ctx.store_init(len(store.tables), shape, store.tau_idx, beta0, dbeta, delta0, ddelta, dtype)
-    for k, T in enumerate(store.tables):
-        if gen is not None and T is None:
-            M, P, Q, S, seed = gen
-            ctx.store_generate_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], M, P, Q, S[k], seed)
-        else:
-            if tuple(np.asarray(T).shape) != shape:
-                raise ValueError("every node table must have the same shape")
-            ctx.store_set_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], T)
+    if gen is not None:
+        for k, T in enumerate(store.tables):
+            if T is None:
+                M, P, Q, S, seed = gen
+                ctx.store_generate_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], M, P, Q, S[k], seed)
+            else:
+                if tuple(np.asarray(T).shape) != shape:
+                    raise ValueError("every node table must have the same shape")
+                ctx.store_set_node(k, store.s[k], store.alpha_lo[k], store.alpha_hi[k], T)
+    else:
+        if any(tuple(np.shape(T)) != shape for T in store.tables):
+            raise ValueError("every node table must have the same shape")
+        files, offs = getattr(store, "files", None), getattr(store, "t_offsets", None)
+        stream = bool(getattr(store, "mapped", False)) and files is not None and offs is not None
+        paths = [f if (stream and o is not None) else None for f, o in zip(files, offs)] if stream else None
+        hosts = [T if (paths is None or paths[k] is None) else None for k, T in enumerate(store.tables)]
+        store.load_stats = ctx.store_load(0, store.s, store.alpha_lo, store.alpha_hi, paths=paths,
+                                          offsets=offs if stream else None, hosts=hosts,
+                                          readers=getattr(store, "readers", 6), direct=getattr(store, "direct", False))
     ctx.store_token = token
     ctx.prep_token = None

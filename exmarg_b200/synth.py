@@ -297,7 +297,7 @@ def write_store(path, spec, s_nodes, seed, n_max=120):
 
 class MemoryStore:
     """a store held in memory with the fields of the reference's RedshiftStore
-    (exmarg/search/store.py:171-181)"""
+    (exmarg/search/store.py:77-87)"""
 
     def __init__(self, spec, s_nodes, seed, tables=None, n_max=120, table_dtype="f32"):
         self.spec = spec

@@ -103,20 +103,38 @@ EXM_API int exm_device_memory(int device, size_t *free_bytes, size_t *total_byte
 /* Declare the store: n_nodes tables of shape (ntau, nphif, nb, nd), stored on the
  * device as `dtype` (EXM_DTYPE_*), lags tau_idx (ntau, in samples), the (beta,
  * Delta) grids beta0 + i dbeta and delta0 + j ddelta shared by every node.
- * Replaces exmarg/search/store.py:204-214 (upload) with resident device tables. */
+ * Replaces exmarg/search/store.py:110-120 (upload) with resident device tables. */
 EXM_API int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, int nb, int nd, int dtype,
                    const int64_t *tau_idx, double beta0, double dbeta, double delta0, double ddelta);
 
 /* Node k: its signal power s and amplitude-axis limits (alpha[0], alpha[-1]), and
  * its float32 table T (ntau, nphif, nb, nd, C order) copied from the host.
- * Replaces one iteration of exmarg/search/store.py:210-212 and the per-node
- * metadata of load_redshift_store (store.py:184-201). */
+ * Replaces one iteration of exmarg/search/store.py:116-117 and the per-node
+ * metadata of load_redshift_store (store.py:90-107). */
 EXM_API int exm_store_set_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi, const float *T);
+
+/* Nodes first .. first+n-1 loaded in one pipelined pass.  Node i's float32 table (ntau, nphif, nb, nd,
+ * C order) is read from the file paths[i] at byte offset offsets[i] (the data of the uncompressed
+ * T.npy member of a bd_*.npz) when paths is non-NULL and paths[i] is set, else copied from the host
+ * array hosts[i].  s, alpha_lo, alpha_hi (n each, s ascending) as exm_store_set_node.
+ * readers: reader threads, 1..64; chunk_bytes: staging chunk (0: 8 MiB; whole rows, at least one);
+ * flags: EXM_LOAD_DIRECT reads files with O_DIRECT (no page cache) where the file system allows it
+ * and with buffered reads elsewhere.  Reads fill a ring of pinned buffers while earlier chunks
+ * are copied to the device; 16-bit stores are quantized on the device per node.
+ * stats_out (8 doubles, may be NULL): seconds, bytes from files, bytes from host arrays, nodes
+ * opened with O_DIRECT, staging buffers, chunk bytes, reader seconds (summed over threads),
+ * seconds the copy issuer waited for reads.
+ * Replaces load_redshift_store's table readers (exmarg/search/store.py:23-74, readers threads)
+ * followed by upload (store.py:110-120). */
+#define EXM_LOAD_DIRECT 1
+EXM_API int exm_store_load(exm_ctx *ctx, int first, int n, const char *const *paths, const int64_t *offsets,
+                           const float *const *hosts, const double *s, const double *alpha_lo, const double *alpha_hi,
+                           int readers, long long chunk_bytes, int flags, double *stats_out);
 
 /* Node k filled on the device by the seeded synthetic generator (the same float32
  * values as exmarg_b200.synth.gen_table_node): T = M[b,d] * P[c] * Q[r] - S + hash
  * perturbation.  M (nb*nd), P (nphif), Q (ntau) float32.  No reference
- * counterpart: it stands in for reading bd_*.npz (store.py:149-168). */
+ * counterpart: it stands in for reading bd_*.npz (store.py:23-74). */
 EXM_API int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alpha_lo, double alpha_hi,
                             const float *M, const float *P, const float *Q, float S, uint32_t seed);
 

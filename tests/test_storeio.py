@@ -1,0 +1,68 @@
+"""The store loader's host side: load_redshift_store records, per node, the file and the byte offset of
+its T.npy data (what exm_store_load reads), and upload_store streams a mapped store from its files and
+sends a store read into memory from its host arrays."""
+
+import numpy as np
+import pytest
+
+import exmarg_b200 as eb
+from exmarg_b200 import synth
+from exmarg_b200.store import upload_store
+
+SPEC = dict(ntau=3, nphif=49, nb=20, nd=13)
+NODES = [5, 17, 30, 44]
+SEED = 7
+
+
+@pytest.fixture(scope="module")
+def store_dir(tmp_path_factory):
+    d = tmp_path_factory.mktemp("bd")
+    spec = synth.TableSpec(**SPEC)
+    s = synth.S_NODES_PROD[NODES]
+    synth.write_store(str(d), spec, s, SEED)
+    return str(d), spec, s
+
+
+class FakeContext:
+    """records what upload_store asks of the device context"""
+    store_token = None
+    prep_token = None
+
+    def store_init(self, *args):
+        self.init = args
+
+    def store_load(self, first, s, alpha_lo, alpha_hi, paths=None, offsets=None, hosts=None, readers=6,
+                   chunk_bytes=0, direct=False):
+        self.load = dict(first=first, s=s, paths=paths, offsets=offsets, hosts=hosts, readers=readers, direct=direct)
+        return {}
+
+
+def test_offsets_point_at_the_tables(store_dir):
+    d, spec, s = store_dir
+    st = eb.load_redshift_store(d, mmap=True)
+    assert np.array_equal(st.s, s)
+    n = int(np.prod(spec.shape))
+    for k, (f, off) in enumerate(zip(st.files, st.t_offsets)):
+        assert off is not None
+        raw = np.fromfile(f, np.float32, count=n, offset=off).reshape(spec.shape)
+        assert np.array_equal(raw, synth.gen_table_node(spec, k, s, SEED))
+        assert np.array_equal(raw, st.tables[k])
+
+
+def test_upload_streams_a_mapped_store(store_dir):
+    d, _, _ = store_dir
+    st = eb.load_redshift_store(d, mmap=True, readers=3, direct=True)
+    ctx = FakeContext()
+    upload_store(st, ctx)
+    assert ctx.load["paths"] == st.files and ctx.load["offsets"] == st.t_offsets
+    assert all(h is None for h in ctx.load["hosts"])
+    assert ctx.load["readers"] == 3 and ctx.load["direct"] is True and ctx.load["first"] == 0
+
+
+def test_upload_sends_host_tables(store_dir):
+    d, _, _ = store_dir
+    st = eb.load_redshift_store(d)
+    ctx = FakeContext()
+    upload_store(st, ctx)
+    assert ctx.load["paths"] is None
+    assert all(h is T for h, T in zip(ctx.load["hosts"], st.tables))
