@@ -329,6 +329,111 @@ def redshift_leg(args, store, seg, local):
             "ln_b_range": [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]}
 
 
+def store_io_leg(args, local):
+    """loading a store into HBM: io_nodes production-shape node files (87 x 49 x 200 x 219 float32,
+    0.75 GB each) written to a temporary directory, then loaded into a fresh context (created and
+    declared before the clock starts) --
+      reference_pattern: as the reference does it, `readers` threads read every table into host
+        memory, then one pageable copy per node;
+      native_files: the native loader streaming the files (buffered reads, reads overlapped with copies);
+      native_files_direct: the same with O_DIRECT (the disk's own rate);
+      native_from_host: the native loader from tables already in host memory.
+    "cold" legs first drop these files' pages from the page cache (fsync, then posix_fadvise
+    DONTNEED on each file), so their reads come from the disk; "hot" legs read the cached pages.
+    Every load is checked bit for bit on its first and last node."""
+    import shutil
+    import tempfile
+    import torch
+    from exmarg_b200 import _lib, synth
+    from exmarg_b200.store import load_redshift_store, store_grid
+    n, R = args.io_nodes, args.io_readers
+    spec = synth.TableSpec()
+    s_nodes = synth.S_NODES_PROD[np.linspace(0, 52, n).astype(int)]
+    d = tempfile.mkdtemp(prefix="exmarg_store_", dir=args.io_dir)
+    out = {"nodes": n, "node_bytes": int(np.prod(spec.shape)) * 4, "readers": R}
+    try:
+        T = np.random.default_rng(1).random(spec.shape, dtype=np.float32)
+        t0 = time.perf_counter()
+        for k, sk in enumerate(s_nodes):
+            T.flat[0] = np.float32(k)
+            np.savez(os.path.join(d, "bd_n120_s%09.3f.npz" % sk), T=T, beta=spec.beta, delta=spec.delta,
+                     tau_idx=spec.tau_idx, alpha=synth.ALPHA, s_node=float(sk))
+        out["write_s"] = time.perf_counter() - t0
+        total = n * out["node_bytes"]
+
+        h = torch.empty(1 << 30, dtype=torch.uint8).pin_memory()       # the host-to-device ceiling
+        g = torch.empty(1 << 30, dtype=torch.uint8, device="cuda:%d" % local)
+        g.copy_(h, non_blocking=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(4):
+            g.copy_(h, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        out["pinned_h2d_GB_per_s"] = 4 * (1 << 30) / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        del h, g
+        torch.cuda.empty_cache()
+
+        def drop_cached():
+            for f in os.listdir(d):
+                fd = os.open(os.path.join(d, f), os.O_RDONLY)
+                try:
+                    os.fsync(fd)
+                    os.posix_fadvise(fd, 0, 0, os.POSIX_FADV_DONTNEED)
+                finally:
+                    os.close(fd)
+
+        def check(ctx):
+            for k in (0, n - 1):
+                T.flat[0] = np.float32(k)
+                if not np.array_equal(ctx.store_get_node(k, spec.shape), T):
+                    raise RuntimeError("store load: node %d differs from its file" % k)
+
+        meta = load_redshift_store(d, mmap=True)
+
+        def leg(kind, cold):
+            ctx = _lib.Context(local)
+            b0, db, d0, dd = store_grid(meta)
+            ctx.store_init(n, spec.shape, meta.tau_idx, b0, db, d0, dd)
+            host = load_redshift_store(d, readers=R) if kind == "host" else None
+            if cold:
+                drop_cached()
+            stats = None
+            t0 = time.perf_counter()
+            if kind == "reference":
+                st = load_redshift_store(d, readers=R)
+                for k in range(n):
+                    ctx.store_set_node(k, st.s[k], st.alpha_lo[k], st.alpha_hi[k], st.tables[k])
+            elif kind == "host":
+                stats = ctx.store_load(0, host.s, host.alpha_lo, host.alpha_hi, hosts=host.tables, readers=R)
+            else:
+                st = load_redshift_store(d, mmap=True)
+                stats = ctx.store_load(0, st.s, st.alpha_lo, st.alpha_hi, paths=st.files, offsets=st.t_offsets,
+                                       readers=R, direct=(kind == "direct"))
+            dt = time.perf_counter() - t0
+            check(ctx)
+            ctx.close()
+            r = {"seconds": dt, "GB_per_s": total / dt / 1e9, "seconds_for_53_nodes": dt * 53.0 / n}
+            if stats is not None:
+                r["reader_seconds"] = stats["read_seconds"]
+                r["issuer_wait_seconds"] = stats["issue_wait_seconds"]
+            return r
+
+        out["legs"] = {
+            "reference_pattern_cold": leg("reference", True),
+            "native_files_cold": leg("files", True),
+            "native_files_direct": leg("direct", True),
+            "reference_pattern_hot": leg("reference", False),
+            "native_files_hot": leg("files", False),
+            "native_from_host": leg("host", False),
+        }
+        out["reference_published"] = "23 s for the 53-node store (39.6 GB), load_redshift_store with 6 readers"
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return out
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
@@ -476,6 +581,8 @@ def run_b200(args):
         line["batched"] = batched_leg(args, store, bank, local)
     if rank == 0 and world == 1 and args.redshift_segments > 0:
         line["redshift"] = redshift_leg(args, store, seg, local)
+    if rank == 0 and world == 1 and args.io_nodes > 0:
+        line["store_io"] = store_io_leg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -522,6 +629,9 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--io-nodes", type=int, default=8, help="node files of the store-loading leg (0: none)")
+    ap.add_argument("--io-readers", type=int, default=6, help="reader threads of the store-loading leg")
+    ap.add_argument("--io-dir", default=None, help="where the store-loading leg writes its files (default: TMPDIR)")
     ap.add_argument("--redshift-segments", type=int, default=8, help="segments of the pe_redshift leg (0: none)")
     ap.add_argument("--batch-segments", type=int, default=16, help="segments of the batched leg (0: none)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
