@@ -14,8 +14,9 @@ from .segments import D0, read_segments
 from .bank import MassBank, mass_bank, from_bank, array_module
 from .store import RedshiftStore, load_redshift_store, quantize_table, upload_store, with_table_dtype
 from .pe import pe_intrinsic, pe_redshift, distance_weights, prepare, autotune
+from .shard import pe_intrinsic_sharded, node_ranges, shard_of
 from ._lib import Context, context
 
 __all__ = ["D0", "read_segments", "MassBank", "mass_bank", "from_bank", "array_module", "RedshiftStore",
-           "load_redshift_store", "upload_store", "quantize_table", "with_table_dtype", "pe_intrinsic", "pe_redshift", "distance_weights", "prepare", "autotune", "Context",
+           "load_redshift_store", "upload_store", "quantize_table", "with_table_dtype", "pe_intrinsic", "pe_redshift", "pe_intrinsic_sharded", "node_ranges", "shard_of", "distance_weights", "prepare", "autotune", "Context",
            "context"]

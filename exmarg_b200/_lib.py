@@ -25,7 +25,7 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame", "exm_store_load")
+           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -78,6 +78,7 @@ def load():
         "exm_redshift_grid": ([P, I, I, P, P, I, P, P, I, P, P], I),
         "exm_source_frame": ([P, P, P, P], I),
         "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
+        "exm_store_set_shard": ([P, D], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -214,6 +215,11 @@ class Context:
                                             int(readers), int(chunk_bytes), LOAD_DIRECT if direct else 0, _p(st)))
         del keep
         return dict(zip(LOAD_STATS, st.tolist()))
+
+    def store_set_shard(self, s_before):
+        """this context's store is a node range of a larger store; s_before: the s of the node below it"""
+        self._check(self.lib.exm_store_set_shard(self.h, float(s_before)))
+        self.prep_token = None
 
     def store_generate_node(self, k, s, alpha_lo, alpha_hi, M, P, Q, S, seed):
         M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))

@@ -274,6 +274,8 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         ctx->alo = parent->alo;
         ctx->ahi = parent->ahi;
         ctx->node_set = parent->node_set;
+        ctx->shard = parent->shard;
+        ctx->s_before = parent->s_before;
         ctx->T.p = parent->T.p;            // borrowed: not counted, not freed
         ctx->tscale = parent->tscale;
         ctx->d_tscale.p = parent->d_tscale.p;
@@ -422,6 +424,8 @@ extern "C" int exm_store_init(exm_ctx *ctx, int n_nodes, int ntau, int nphif, in
     REQUIRE(dbeta > 0 && ddelta > 0, EXM_ERR_ARG, "grid steps must be positive");
     ctx->store_ok = ctx->prep_ok = false;
     ctx->tmap_ok = false;
+    ctx->shard = false;
+    ctx->s_before = 0.0;
     ctx->nn = n_nodes;
     ctx->ntau = ntau;
     ctx->nphif = nphif;
@@ -520,6 +524,20 @@ extern "C" int exm_store_load(exm_ctx *ctx, int first, int n, const char *const 
     if (first > 0 && ctx->node_set[first - 1]) REQUIRE(s[0] > ctx->s[first - 1], EXM_ERR_ARG, "nodes must be added with s ascending");
     exm_store_load_run(ctx, first, n, paths, offsets, hosts, readers, chunk_bytes, flags, stats_out);
     for (int i = 0; i < n; ++i) set_node_meta(ctx, first + i, s[i], alpha_lo[i], alpha_hi[i]);
+    API_END(ctx)
+}
+
+extern "C" int exm_store_set_shard(exm_ctx *ctx, double s_before)
+{
+    API_BEGIN(ctx)
+    REQUIRE(!ctx->store_borrowed, EXM_ERR_STATE, "this context borrows its parent's store");
+    REQUIRE(ctx->n_children.load() == 0, EXM_ERR_STATE, "child contexts borrow this store: destroy them first");
+    REQUIRE(ctx->T.p, EXM_ERR_STATE, "exm_store_init first");
+    REQUIRE(s_before >= 0.0 && std::isfinite(s_before), EXM_ERR_ARG, "s_before must be finite and >= 0");
+    REQUIRE(!ctx->node_set[0] || s_before < ctx->s[0], EXM_ERR_ARG, "s_before must lie below the shard's first node");
+    ctx->shard = true;
+    ctx->s_before = s_before;
+    ctx->prep_ok = false;
     API_END(ctx)
 }
 
@@ -634,7 +652,7 @@ extern "C" int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double
     std::vector<double> blna(nm, 0.0);
     for (int k = 0; k < nn; ++k) {
         const double alo = std::min(ctx->alo[k], ymin * ymin);
-        const double s_prev = k > 0 ? ctx->s[k - 1] : 0.0;
+        const double s_prev = k > 0 ? ctx->s[k - 1] : ctx->s_before;
         const double a_b = alo * (1.0 + 1e-9);
         for (int m = 0; m < nm; ++m) {
             const double a = ctx->s[k] / ctx->u[m];
@@ -648,7 +666,7 @@ extern "C" int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double
             }
         }
     }
-    for (int m = 0; m < nm; ++m) {
+    for (int m = 0; m < nm && !ctx->shard; ++m) {   // a shard's templates may reach its nodes 0 or 1 times
         int pts = 0;
         for (int k = 0; k <= nn; ++k) pts += y[(size_t)k * nm + m] > 0;
         if (pts < 2) {
@@ -952,6 +970,7 @@ extern "C" int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, cons
     API_BEGIN(ctx)
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(ctx->prep_ok, EXM_ERR_STATE, "exm_pe_prepare first");
+    REQUIRE(!ctx->shard, EXM_ERR_STATE, "a store shard gives node values (exm_node_values); ln Lambda needs every shard's");
     REQUIRE(n_seg >= 0 && d_H && d_L && sig2_H && sig2_L && ln_lambda && ln_b, EXM_ERR_ARG, "null argument");
     REQUIRE(n_loud == 0 || seeds, EXM_ERR_ARG, "seeds are needed when n_loud > 0");
     const RunShape rs = run_shape(ctx, n_loud, n_random);

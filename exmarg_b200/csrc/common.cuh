@@ -84,6 +84,8 @@ struct exm_ctx {
 
     // store (a child context borrows its parent's: it neither fills nor frees it)
     bool store_ok = false, store_borrowed = false;
+    bool shard = false;         // the store is a contiguous node range of a larger store
+    double s_before = 0.0;      // s of the node just below that range (0: it starts at the first node)
     exm_ctx *parent = nullptr;              // the context whose store this one borrows
     std::atomic<int> n_children{0};         // child contexts borrowing this context's store
     bool destroy_pending = false;           // destroyed while children were alive: freed with the last one

@@ -199,5 +199,8 @@ def upload_store(store, ctx):
         store.load_stats = ctx.store_load(0, store.s, store.alpha_lo, store.alpha_hi, paths=paths,
                                           offsets=offs if stream else None, hosts=hosts,
                                           readers=getattr(store, "readers", 6), direct=getattr(store, "direct", False))
+    s_before = getattr(store, "shard_s_before", None)
+    if s_before is not None:
+        ctx.store_set_shard(s_before)
     ctx.store_token = token
     ctx.prep_token = None

@@ -131,6 +131,16 @@ EXM_API int exm_store_load(exm_ctx *ctx, int first, int n, const char *const *pa
                            const float *const *hosts, const double *s, const double *alpha_lo, const double *alpha_hi,
                            int readers, long long chunk_bytes, int flags, double *stats_out);
 
+/* Declare the context's store a shard: a contiguous range of the nodes of a larger store, the node
+ * just below the range having signal power s_before (0 when the range starts at the first node).
+ * exm_pe_prepare then sets the boundary point of the range's first node as the whole store would
+ * (exmarg/search/pe.py:75-81 with s_prev = s_before) and accepts templates that reach fewer than
+ * two of the shard's nodes; exm_node_values gives the whole store's rows for these nodes (and its
+ * boundary row for templates whose boundary node is here, -inf elsewhere).  exm_pe_intrinsic
+ * refuses a shard: the node log-sum-exp needs every shard's rows and the whole store's weights.
+ * exm_store_init clears the setting.  No reference counterpart: node sharding across GPUs. */
+EXM_API int exm_store_set_shard(exm_ctx *ctx, double s_before);
+
 /* Node k filled on the device by the seeded synthetic generator (the same float32
  * values as exmarg_b200.synth.gen_table_node): T = M[b,d] * P[c] * Q[r] - S + hash
  * perturbation.  M (nb*nd), P (nphif), Q (ntau) float32.  No reference
