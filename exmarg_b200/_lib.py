@@ -25,7 +25,7 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard")
+           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -79,6 +79,7 @@ def load():
         "exm_source_frame": ([P, P, P, P], I),
         "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
         "exm_store_set_shard": ([P, D], I),
+        "exm_bd_build": ([P, I, I, I, I, P, P, P, I, P, I, P, P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -220,6 +221,26 @@ class Context:
         """this context's store is a node range of a larger store; s_before: the s of the node below it"""
         self._check(self.lib.exm_store_set_shard(self.h, float(s_before)))
         self.prep_token = None
+
+    def bd_build(self, col, row, lnq, beta, ladder):
+        """stage 3 of the table build: (T (n_ladder, ntau, nphif, nb, 2 nq - 1) float32, entries not
+        finite, (kernel ms, ms with copies))"""
+        col = np.ascontiguousarray(col, np.float32)
+        row = np.ascontiguousarray(row, np.float32)
+        if col.ndim != 4 or col.shape != row.shape:
+            raise ValueError("col and row must both be (orders, lags, nq, phases)")
+        nord, ntau, nq, nphif = col.shape
+        lnq = np.ascontiguousarray(lnq, np.float64)
+        beta = np.ascontiguousarray(beta, np.float64)
+        lad = np.ascontiguousarray(ladder, np.int32)
+        if lnq.size != nq:
+            raise ValueError("lnq must have one entry per magnitude")
+        T = np.empty((lad.size, ntau, nphif, beta.size, 2 * nq - 1), np.float32)
+        bad = ctypes.c_longlong(0)
+        ms = np.zeros(2)
+        self._check(self.lib.exm_bd_build(self.h, nord, ntau, nq, nphif, _p(col), _p(row), _p(lnq), beta.size, _p(beta),
+                                          lad.size, _p(lad), _p(T), ctypes.byref(bad), _p(ms)))
+        return T, int(bad.value), (float(ms[0]), float(ms[1]))
 
     def store_generate_node(self, k, s, alpha_lo, alpha_hi, M, P, Q, S, seed):
         M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))

@@ -152,6 +152,21 @@ EXM_API int exm_store_generate_node(exm_ctx *ctx, int k, double s, double alpha_
  * 16-bit storage).  For tests. */
 EXM_API int exm_store_get_node(exm_ctx *ctx, int k, float *T_out);
 
+/* ------------------------------------------------------------------ table build */
+
+/* Stage 3 of the offline table build (scripts/build_tables/build_bd.py:53-77): one node's table
+ * T[tau, phi, beta, Delta] = log sum_{n <= n_max} exp(n beta + g_n(Delta)), float64 arithmetic,
+ * float32 result, for each truncation order n_max in ladder (n_ladder of them).
+ * col, row: float32 (nord, ntau, nq, nphif), the last column lnK[n, tau, :, nq-1, :nphif] and the
+ * last row lnK[n, tau, nq-1, :, :nphif] of stage 2's lnK (nord orders, nq magnitudes);
+ * lnq (nq) the log magnitudes, beta (nb) the beta grid.  T_out: n_ladder tables of
+ * (ntau, nphif, nb, 2 nq - 1) float32, Delta ascending as build_bd.py:57 orders it.
+ * n_nonfinite_out: entries that are not finite (the reference then refuses the table);
+ * ms_out (may be NULL): kernel milliseconds, milliseconds including the copies. */
+EXM_API int exm_bd_build(exm_ctx *ctx, int nord, int ntau, int nq, int nphif, const float *col, const float *row,
+                         const double *lnq, int nb, const double *beta, int n_ladder, const int *ladder,
+                         float *T_out, long long *n_nonfinite_out, double *ms_out);
+
 /* ------------------------------------------------------------------ bank */
 
 /* The template bank: nm templates of nfreq complex64 factors W = a e^{i psi0}

@@ -420,3 +420,35 @@ def pe_redshift(seg, W, u, M, lo, n_time, store, dl_of_z, zmax=8.0, nz=1600, m1_
     w = redshift_weights(m1, z, dl, mdet_range)
     ln_b = np.array([log_mean(L, w) for L in out])
     return dict(m1=m1, z=z, ln_lambda=out, ln_b=ln_b)
+
+
+# ----------------------------------------------------------------------------- table build, stage 3
+
+def bd_tables(col, row, lnq, beta, ladder):
+    """scripts/build_tables/build_bd.py:53-77: T_nm[tau, phi, b, d] = log sum_{n <= nm} exp(n beta_b + g_n(Delta_d))
+    for each truncation order nm, float64 arithmetic rounded to float32.
+
+    col, row: (orders, lags, nq, nphif) -- lnK on the last column (q2 = q_last) and the last row (q1 = q_last);
+    g_n on Delta <= 0 is col - 2n ln q_last (Delta ascending with q1), on Delta > 0 row - 2n ln q2 (q2 descending)."""
+    col = np.asarray(col, np.float64)
+    row = np.asarray(row, np.float64)
+    lnq = np.asarray(lnq, np.float64)
+    beta = np.asarray(beta, np.float64)
+    nord, ntau, nq, nphif = col.shape
+    n = np.arange(nord, dtype=np.float64)
+    two_n = 2.0 * n
+    out = {nm: np.empty((ntau, nphif, beta.size, 2 * nq - 1), np.float32) for nm in ladder}
+    nbeta = n[:, None] * beta[None, :]                                   # (orders, nb)
+    for t in range(ntau):
+        lo = col[:, t] - (two_n * lnq[-1])[:, None, None]               # (orders, nq, nphif), q1 ascending
+        hi = row[:, t] - two_n[:, None, None] * lnq[None, :, None]      # q2 ascending
+        g = np.concatenate([lo, hi[:, -2::-1]], axis=1)                 # (orders, 2 nq - 1, nphif)
+        for p in range(nphif):
+            E = nbeta[:, :, None] + g[None, :, :, p].transpose(1, 0, 2)   # (orders, nb, nd)
+            for nm in ladder:
+                mx = E[:nm + 1].max(axis=0)
+                tot = np.zeros_like(mx)
+                for k in range(nm + 1):                                  # in order of n
+                    tot += np.exp(E[k] - mx)
+                out[nm][t, p] = (mx + np.log(tot)).astype(np.float32)
+    return out

@@ -1,5 +1,6 @@
 """Golden vectors for the pe_intrinsic path, produced by running the REFERENCE's own CPU
-code (exmarg.search: numpy + numba) in a container where its source tree is present.
+code (exmarg.search: numpy + numba; and its table builder scripts/build_tables/build_bd.py)
+in a container where its source tree is present.
 
     python tests/golden/make_golden.py [reference src dir [case ...]]
 
@@ -139,16 +140,68 @@ def make_redshift(name, c, search):
           "size %.1f MB" % (os.path.getsize(os.path.join(HERE, "%s.npz" % name)) / 1e6))
 
 
+# stage 3 of the table build: a synthetic stage-2 store (lnK of a few orders on a small (q1, q2, phi)
+# grid) through the reference's scripts/build_tables/build_bd.py build_node, full order and a ladder
+BD_CASES = {
+    "bd1": dict(nord=9, ntau=3, nq=12, nphi=8, s=1.0, seed=11, ladder=(2, 5, 8)),
+}
+
+
+def synthetic_lnk(c):
+    """lnK_n(tau, q1, q2, phi), float32: homogeneous of degree 2n in (q1, q2) (2n ln max(q1, q2) plus a
+    function of ln q1 - ln q2), a Poisson-like fall-off in n, smooth in tau and phi, a little noise"""
+    rng = np.random.default_rng(c["seed"])
+    lnq = np.log(np.geomspace(0.05, 100.0, c["nq"]))
+    n = np.arange(c["nord"], dtype=np.float64)[:, None, None, None, None]
+    t = np.arange(c["ntau"], dtype=np.float64)[None, :, None, None, None]
+    l1 = lnq[None, None, :, None, None]
+    l2 = lnq[None, None, None, :, None]
+    ph = (2 * np.pi * np.arange(c["nphi"]) / c["nphi"])[None, None, None, None, :]
+    from scipy.special import gammaln
+    A = (2 * n * np.maximum(l1, l2) + n * (0.4 * np.cos(ph) + 0.1 * t - 0.3 * np.abs(l1 - l2)) - gammaln(n + 1.0)
+         + 0.01 * rng.standard_normal((c["nord"], c["ntau"], c["nq"], c["nq"], c["nphi"])))
+    return A.astype(np.float32), lnq
+
+
+def make_bd(name, c, ref_root):
+    import importlib.util
+    import tempfile
+    A, lnq = synthetic_lnk(c)
+    tau_idx = np.arange(c["ntau"]) - c["ntau"] // 2
+    with tempfile.TemporaryDirectory() as d:
+        stem = os.path.join(d, "kstore_n%03d_s%09.3f" % (c["nord"] - 1, c["s"]))
+        np.save(stem + ".lnK.npy", A)
+        np.savez(stem + ".meta.npz", s_node=c["s"], lnq=lnq, tau_idx=tau_idx)
+        os.environ["BD_NMAX_LADDER"] = ",".join(str(v) for v in c["ladder"])
+        spec = importlib.util.spec_from_file_location("build_bd", os.path.join(ref_root, "scripts", "build_tables",
+                                                                              "build_bd.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        base = os.path.join(d, "bd")
+        mod.build_node(stem, base)
+        out = dict(lnK=A, lnq=lnq, tau_idx=tau_idx, s=c["s"], ladder=np.array(c["ladder"]))
+        for nm in c["ladder"]:
+            z = np.load(os.path.join(mod.out_dir(base, nm, c["nord"] - 1), "bd_n%03d_s%09.3f.npz" % (nm, c["s"])))
+            out["T%d" % nm] = z["T"]
+            out["beta"], out["delta"] = z["beta"], z["delta"]
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
-    search = refimport.import_reference(src)
     only = sys.argv[2:] if len(sys.argv) > 2 else None
-    for name, c in CASES.items():
+    if only is None or any(n in only for n in list(CASES) + list(REDSHIFT_CASES)):
+        search = refimport.import_reference(src)
+        for name, c in CASES.items():
+            if only is None or name in only:
+                make(name, c, search)
+        for name, c in REDSHIFT_CASES.items():
+            if only is None or name in only:
+                make_redshift(name, c, search)
+    for name, c in BD_CASES.items():
         if only is None or name in only:
-            make(name, c, search)
-    for name, c in REDSHIFT_CASES.items():
-        if only is None or name in only:
-            make_redshift(name, c, search)
+            make_bd(name, c, os.path.dirname(os.path.abspath(src)))
 
 
 if __name__ == "__main__":
