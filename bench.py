@@ -449,6 +449,47 @@ def store_io_leg(args, local):
     return out
 
 
+def table_build_leg(args, local):
+    """stage 3 of the offline table build for one production-shape node: 121 orders (n_max 120), 87 lags,
+    110 magnitudes (200 x 219 table), 49 phases, synthetic lnK edges.  Device: exm_bd_build (kernel time
+    and time with the host copies), median of 3.  CPU baseline: the reference's algorithm (numpy, float64,
+    the restatement in oracle/) on one lag, scaled by the 87 lags."""
+    from scipy.special import gammaln
+    from exmarg_b200 import _lib, tables
+    nord, ntau, nq, nphif = 121, 87, 110, 49
+    rng = np.random.default_rng(5)
+    lnq = np.log(np.geomspace(0.05, 100.0, nq))
+    n = np.arange(nord, dtype=np.float64)[:, None, None, None]
+    t = np.arange(ntau, dtype=np.float64)[None, :, None, None]
+    ph = (2 * np.pi * np.arange(nphif) / 96.0)[None, None, None, :]
+    dq = np.abs(lnq - lnq[-1])[None, None, :, None]
+    base = n * (0.4 * np.cos(ph) + 0.01 * t - 0.3 * dq) - gammaln(n + 1.0)
+    col = (2 * n * lnq[-1] + base + 0.01 * rng.standard_normal(base.shape)).astype(np.float32)
+    row = (2 * n * lnq[None, None, :, None] + base + 0.01 * rng.standard_normal(base.shape)).astype(np.float32)
+    ctx = _lib.context(local)
+    beta, _ = tables.bd_grid(lnq)
+    runs = []
+    for _ in range(4):
+        T, bad, ms = ctx.bd_build(col, row, lnq, beta, [nord - 1])
+        runs.append(ms)
+    runs = sorted(runs[1:], key=lambda m: m[0])
+    k_ms, all_ms = runs[1]
+    nout = ntau * nphif * beta.size * (2 * nq - 1)
+    out = {"orders": nord, "lags": ntau, "table": [ntau, nphif, int(beta.size), 2 * nq - 1], "kernel_ms": k_ms,
+           "ms_with_copies": all_ms, "non_finite": bad, "exp_per_s": nout * nord / (k_ms * 1e-3),
+           "seconds_for_53_nodes": all_ms * 1e-3 * 53}
+    if not args.no_cpu:
+        from oracle import restate
+        t0 = time.perf_counter()
+        ref = restate.bd_tables(col[:, :1], row[:, :1], lnq, beta, [nord - 1])[nord - 1]
+        cpu_lag = time.perf_counter() - t0
+        d = np.abs(ref.astype(np.float64) - T[0, 0].astype(np.float64))
+        out["cpu_baseline"] = {"seconds_per_node": cpu_lag * ntau, "cores": 1, "kind": "port",
+                               "sample": "lag 0 of 87 (49 phases x 200 x 219 x 121 orders), scaled by 87"}
+        out["max_abs_diff_vs_cpu_lag0"] = float(d.max())
+    return out
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
@@ -598,6 +639,8 @@ def run_b200(args):
         line["redshift"] = redshift_leg(args, store, seg, local)
     if rank == 0 and world == 1 and args.io_nodes > 0:
         line["store_io"] = store_io_leg(args, local)
+    if rank == 0 and world == 1 and args.table_build:
+        line["table_build"] = table_build_leg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -644,6 +687,7 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--table-build", type=int, default=1, help="run the table-build (stage 3) leg (0: no)")
     ap.add_argument("--io-nodes", type=int, default=8, help="node files of the store-loading leg (0: none)")
     ap.add_argument("--io-readers", type=int, default=6, help="reader threads of the store-loading leg")
     ap.add_argument("--io-dir", default=None, help="where the store-loading leg writes its files (default: TMPDIR)")
