@@ -25,7 +25,7 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build")
+           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -80,6 +80,7 @@ def load():
         "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
         "exm_store_set_shard": ([P, D], I),
         "exm_bd_build": ([P, I, I, I, I, P, P, P, I, P, I, P, P, P, P], I),
+        "exm_w_build": ([P, I, P, I, I, I, P, P, P, P, P, I, P, P, P, I, P, P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -241,6 +242,27 @@ class Context:
         self._check(self.lib.exm_bd_build(self.h, nord, ntau, nq, nphif, _p(col), _p(row), _p(lnq), beta.size, _p(beta),
                                           lad.size, _p(lad), _p(T), ctypes.byref(bad), _p(ms)))
         return T, int(bad.value), (float(ms[0]), float(ms[1]))
+
+    def w_build(self, s_nodes, n_max, g, scale):
+        """stage 1 of the table build over the pixels of geometry g (exmarg_b200.wtable.geometry): W
+        (n_nodes, n_tau, n_keys) float32 and (milliseconds of the quadrature, milliseconds in all)"""
+        s_nodes = np.ascontiguousarray(s_nodes, np.float64)
+        n_keys = (n_max + 1) * (n_max + 2) * (n_max + 3) // 6
+        scale = np.ascontiguousarray(scale, np.float64)
+        if scale.shape != (s_nodes.size, n_keys):
+            raise ValueError("scale must be (nodes, keys)")
+        arr = {k: np.ascontiguousarray(g[k]) for k in ("resp", "j0", "w", "c2p", "s2p", "ap", "cg", "wq")}
+        n_tau = int(g["tau"].size)
+        W = np.empty((s_nodes.size, n_tau, n_keys), np.float32)
+        bad = ctypes.c_longlong(0)
+        ms = np.zeros(2)
+        self._check(self.lib.exm_w_build(self.h, s_nodes.size, _p(s_nodes), int(n_max), arr["c2p"].size, arr["ap"].size,
+                                         _p(arr["c2p"]), _p(arr["s2p"]), _p(arr["ap"]), _p(arr["cg"]), _p(arr["wq"]),
+                                         arr["resp"].shape[0], _p(arr["resp"]), _p(arr["j0"]), _p(arr["w"]), n_tau,
+                                         _p(scale), _p(W), ctypes.byref(bad), _p(ms)))
+        if bad.value:
+            raise FloatingPointError("conditional W table non-finite")
+        return W, (float(ms[0]), float(ms[1]))
 
     def store_generate_node(self, k, s, alpha_lo, alpha_hi, M, P, Q, S, seed):
         M, P, Q = (np.ascontiguousarray(x, np.float32) for x in (M, P, Q))

@@ -167,6 +167,21 @@ EXM_API int exm_bd_build(exm_ctx *ctx, int nord, int ntau, int nq, int nphif, co
                          const double *lnq, int nb, const double *beta, int n_ladder, const int *ladder,
                          float *T_out, long long *n_nonfinite_out, double *ms_out);
 
+/* Stage 1 of the offline table build (scripts/build_tables/w_gpu.py:67-182): the GORFs at fixed
+ * distance W_j(tau, key) at n_nodes nodes s_nodes, keys (n, a, b), b <= a <= n <= n_max, in the order
+ * n, a, b ascending, by quadrature over n_pix sky pixels and the (psi, chi) grid, float64, result
+ * float32 (n_nodes, n_tau, n_keys) in W_out.
+ * c2p, s2p (n_psi) float32 cos 2psi, sin 2psi; ap, cg (n_chi) float32 (1 + chi^2)/2 and chi;
+ * wq (n_chi) float64 quadrature weights; resp (n_pix, 4) float32 F+_H, Fx_H, F+_L, Fx_L at psi = 0;
+ * j0 (n_pix) the lower delay bin of each pixel, w (n_pix, 2) its deposit weights on bins j0, j0 + 1;
+ * scale (n_nodes, n_keys) the per-(node, order) factor s^n 2^n / n!.
+ * n_nonfinite_out: entries that are not finite; ms_out (may be NULL): quadrature milliseconds,
+ * milliseconds in all.  Replaces w_table_s_gpu (w_gpu.py:134-182) with one pixel per step. */
+EXM_API int exm_w_build(exm_ctx *ctx, int n_nodes, const double *s_nodes, int n_max, int n_psi, int n_chi,
+                        const float *c2p, const float *s2p, const float *ap, const float *cg, const double *wq,
+                        int n_pix, const float *resp, const int *j0, const double *w, int n_tau, const double *scale,
+                        float *W_out, long long *n_nonfinite_out, double *ms_out);
+
 /* ------------------------------------------------------------------ bank */
 
 /* The template bank: nm templates of nfreq complex64 factors W = a e^{i psi0}

@@ -452,3 +452,57 @@ def bd_tables(col, row, lnq, beta, ladder):
                     tot += np.exp(E[k] - mx)
                 out[nm][t, p] = (mx + np.log(tot)).astype(np.float32)
     return out
+
+
+# ----------------------------------------------------------------------------- table build, stage 1
+
+def w_table_s(s_nodes, n_max, nside, n_tau, pix2ang, rounding="numpy"):
+    """scripts/build_tables/w_gpu.py:104-182 (the GORFs at fixed distance), float64 numpy, pixel by pixel:
+    responses in float32 as the reference forms them (complex64), |R|^2 and arg R in float32, then ladders,
+    damping and the per-key quadrature sums in float64, the linear delay deposit and the s^n 2^n / n! scale.
+    rounding: 'numpy' takes |R| and arg R from numpy's float32 abs and angle (as the reference run on numpy
+    does); 'correct' rounds them to float32 from float64 (the float32 functions of numpy, CUDA and a
+    correctly rounded evaluation differ in the last bit).
+    Returns tau, W (n_nodes, n_tau, n_keys) float64 over the keys (n, a, b), b <= a, in order."""
+    from scipy.special import gammaln
+    from exmarg_b200 import wtable as wt
+    s = np.atleast_1d(np.asarray(s_nodes, float))
+    psi, cg, wq = wt.quadrature(n_max)
+    tau = wt.tau_grid(n_tau)
+    npix = 12 * nside * nside
+    th, ph = pix2ang(nside, np.arange(npix))
+    j0, w = wt.deposit(tau, th, ph, npix)
+    ks = wt.keys(n_max)
+    c2p, s2p = np.cos(2 * psi).astype(np.float32), np.sin(2 * psi).astype(np.float32)
+    Ap, cgf = (0.5 * (1 + cg ** 2)).astype(np.float32), cg.astype(np.float32)
+    Wraw = np.zeros((s.size, n_tau, len(ks)))
+    for p in range(npix):
+        R = []
+        for I in "HL":
+            fp, fx = wt.antenna(I, th[p:p + 1], ph[p:p + 1])
+            fp, fx = np.float32(fp[0]), np.float32(fx[0])
+            Fp = fp * c2p - fx * s2p
+            Fx = fp * s2p + fx * c2p
+            R.append((Ap[None, :] * Fp[:, None] + 1j * cgf[None, :] * Fx[:, None]).astype(np.complex64).ravel())
+        if rounding == "correct":
+            re = [r.real.astype(np.float64) for r in R]
+            im = [r.imag.astype(np.float64) for r in R]
+            mag = [np.sqrt(a * a + b * b).astype(np.float32) for a, b in zip(re, im)]
+            ang = [np.arctan2(b, a).astype(np.float32) for a, b in zip(re, im)]
+        else:
+            mag = [np.abs(r) for r in R]
+            ang = [np.angle(r) for r in R]
+        S1, S2 = ((mg * mg).astype(np.float64) for mg in mag)
+        dph = (ang[0] - ang[1]).astype(np.float64)
+        m1, m2 = np.sqrt(S1 / 2.0), np.sqrt(S2 / 2.0)
+        wqf = np.broadcast_to(wq[None, :], (psi.size, cg.size)).ravel()
+        Bw = np.stack([np.exp(-(sj * S1 + sj * S2)) for sj in s]) * wqf[None, :]        # (nodes, Q)
+        V = np.empty((s.size, len(ks)))
+        for k, (n, a, b) in enumerate(ks):
+            V[:, k] = (Bw * np.cos((a - b) * dph)[None, :]) @ (m1 ** (a + b) * m2 ** (2 * n - a - b))
+        Wraw[:, j0[p]] += w[p, 0] * V
+        Wraw[:, j0[p] + 1] += w[p, 1] * V
+    n_key = np.array([k[0] for k in ks], float)
+    scale = np.exp(np.minimum(n_key[None, :] * np.log(s)[:, None] - gammaln(n_key + 1.0)[None, :]
+                              + n_key[None, :] * np.log(2.0), 700.0))
+    return tau, Wraw * scale[:, None, :]

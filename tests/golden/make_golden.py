@@ -1,6 +1,6 @@
 """Golden vectors for the pe_intrinsic path, produced by running the REFERENCE's own CPU
-code (exmarg.search: numpy + numba; and its table builder scripts/build_tables/build_bd.py)
-in a container where its source tree is present.
+code (exmarg.search: numpy + numba; its table builders scripts/build_tables/build_bd.py and
+w_gpu.py, the latter with numpy standing in for cupy) in a container where its source tree is present.
 
     python tests/golden/make_golden.py [reference src dir [case ...]]
 
@@ -188,6 +188,38 @@ def make_bd(name, c, ref_root):
     print(name, {k: v.shape for k, v in out.items() if hasattr(v, "shape")})
 
 
+# stage 1 of the table build: the reference's scripts/build_tables/w_gpu.py w_table_s_gpu on a small sky,
+# run with numpy in place of cupy and exmarg_b200.wtable's HEALPix pixel centres in place of healpy
+W_CASES = {
+    "w1": dict(s=(0.5, 3.0, 20.0), n_max=4, nside=2, n_tau=17, chunk=7),
+}
+
+
+def make_w(name, c, ref_root):
+    import importlib.util
+    import types
+    from exmarg_b200 import wtable
+    cp = types.ModuleType("cupy")
+    cp.__dict__.update({k: getattr(np, k) for k in dir(np) if not k.startswith("_")})
+    cp.asnumpy = np.asarray
+    cp.cuda = types.SimpleNamespace(Stream=types.SimpleNamespace(null=types.SimpleNamespace(synchronize=lambda: None)))
+    sys.modules["cupy"] = cp
+    hp = sys.modules.get("healpy") or types.ModuleType("healpy")
+    hp.nside2npix = wtable.nside2npix
+    hp.pix2ang = wtable.pix2ang
+    sys.modules["healpy"] = hp
+    spec = importlib.util.spec_from_file_location("w_gpu", os.path.join(ref_root, "scripts", "build_tables", "w_gpu.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    s = np.array(c["s"], float)
+    tau, W = mod.w_table_s_gpu(s, s, c["n_max"], n_tau=c["n_tau"], nside=c["nside"], chunk=c["chunk"])
+    keys = wtable.keys(c["n_max"])
+    out = np.array([[Wj[k] for k in keys] for Wj in W])            # (nodes, keys, tau)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), s=s, n_max=c["n_max"], nside=c["nside"], n_tau=c["n_tau"],
+                        tau=tau, W=np.ascontiguousarray(out.transpose(0, 2, 1)))
+    print(name, out.shape, float(np.abs(out).max()))
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
     only = sys.argv[2:] if len(sys.argv) > 2 else None
@@ -202,6 +234,10 @@ def main():
     for name, c in BD_CASES.items():
         if only is None or name in only:
             make_bd(name, c, os.path.dirname(os.path.abspath(src)))
+    for name, c in W_CASES.items():
+        if only is None or name in only:
+            refimport.import_reference(src)          # exmarg on the path, with its stub modules
+            make_w(name, c, os.path.dirname(os.path.abspath(src)))
 
 
 if __name__ == "__main__":
