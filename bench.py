@@ -490,6 +490,53 @@ def table_build_leg(args, local):
     return out
 
 
+def w_build_leg(args, local):
+    """stage 1 of the offline table build at the published settings (n_max 120, nside 32: 12288 pixels,
+    257 delays, 53 nodes; 302621 keys, 243 x 123 quadrature points): exm_w_build on w_pixels pixels spread
+    over the sky, the whole build projected from the time per pixel (the pixels are independent and
+    equally costly).  CPU baseline: the reference's per-key quadrature (numpy, float64) for a sample of
+    keys of one pixel, scaled to a pixel."""
+    from exmarg_b200 import wtable, _lib, synth
+    s_nodes = synth.S_NODES_PROD
+    npix = wtable.nside2npix(wtable.NSIDE)
+    pix = np.linspace(0, npix - 1, args.w_pixels).astype(int)
+    g = wtable.geometry(wtable.NSIDE, wtable.N_MAX, wtable.N_TAU, pix)
+    sc = wtable.scales(s_nodes, wtable.N_MAX)
+    ctx = _lib.context(local)
+    W, ms = ctx.w_build(s_nodes, wtable.N_MAX, g, sc)
+    per_px = ms[0] / pix.size
+    q = 243 * 123
+    fma = 53 * q * float(sc.shape[1])
+    out = {"pixels_run": int(pix.size), "ms_per_pixel": per_px, "projected_build_s": per_px * 1e-3 * npix,
+           "reference_published_s": 7.1 * 3600, "reference_published": "7.1 h for the 53 nodes on one GPU (build_w.py:5-6)",
+           "fp64_fma_per_pixel": fma, "fp64_tflops": 2 * fma / (per_px * 1e-3) / 1e12, "ms_with_copies": ms[1],
+           "finite": bool(np.isfinite(W).all())}
+    if not args.no_cpu:
+        th, ph = wtable.pix2ang(wtable.NSIDE, pix[:1])
+        psi, cg, wq = wtable.quadrature(wtable.N_MAX)
+        R = []
+        for I in "HL":
+            fp, fx = (np.float32(v[0]) for v in wtable.antenna(I, th, ph))
+            c2, s2 = np.cos(2 * psi).astype(np.float32), np.sin(2 * psi).astype(np.float32)
+            Fp, Fx = fp * c2 - fx * s2, fp * s2 + fx * c2
+            R.append((np.float32(0.5) * (1 + cg.astype(np.float32) ** 2)[None, :] * Fp[:, None]
+                      + 1j * cg.astype(np.float32)[None, :] * Fx[:, None]).astype(np.complex64).ravel())
+        S1, S2 = (np.abs(r).astype(np.float64) ** 2 for r in R)
+        dph = (np.angle(R[0]) - np.angle(R[1])).astype(np.float64)
+        m1, m2 = np.sqrt(S1 / 2), np.sqrt(S2 / 2)
+        wqf = np.broadcast_to(wq[None, :], (psi.size, cg.size)).ravel()
+        ks = wtable.keys(wtable.N_MAX)
+        sample = ks[::max(1, len(ks) // 200)]
+        t0 = time.perf_counter()
+        Bw = np.stack([np.exp(-(sj * S1 + sj * S2)) for sj in s_nodes]) * wqf[None, :]
+        for (n, a, b) in sample:
+            (Bw * np.cos((a - b) * dph)[None, :]) @ (m1 ** (a + b) * m2 ** (2 * n - a - b))
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"seconds_per_pixel": dt * len(ks) / len(sample), "cores": 1, "kind": "port",
+                               "sample": "%d of %d keys of one pixel, scaled" % (len(sample), len(ks))}
+    return out
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
@@ -641,6 +688,8 @@ def run_b200(args):
         line["store_io"] = store_io_leg(args, local)
     if rank == 0 and world == 1 and args.table_build:
         line["table_build"] = table_build_leg(args, local)
+    if rank == 0 and world == 1 and args.w_pixels > 0:
+        line["w_build"] = w_build_leg(args, local)
     if rank == 0 and world == 1 and not args.no_cpu:
         # CPU baseline and parity: the oracle on a template sample of the first timed segment
         store_h = host_store(spec, s_nodes)
@@ -687,6 +736,7 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--w-pixels", type=int, default=4, help="sky pixels of the stage-1 table-build leg (0: none)")
     ap.add_argument("--table-build", type=int, default=1, help="run the table-build (stage 3) leg (0: no)")
     ap.add_argument("--io-nodes", type=int, default=8, help="node files of the store-loading leg (0: none)")
     ap.add_argument("--io-readers", type=int, default=6, help="reader threads of the store-loading leg")
