@@ -496,8 +496,9 @@ def w_build_leg(args, local):
     over the sky, the whole build projected from the time per pixel (the pixels are independent and
     equally costly).  CPU baseline: the reference's per-key quadrature (numpy, float64) for a sample of
     keys of one pixel, scaled to a pixel."""
+    import torch
     from exmarg_b200 import wtable, _lib, synth
-    s_nodes = synth.S_NODES_PROD
+    s_nodes = synth.S_NODES_PROD[np.linspace(0, 52, min(53, args.w_nodes)).astype(int)]
     npix = wtable.nside2npix(wtable.NSIDE)
     pix = np.linspace(0, npix - 1, args.w_pixels).astype(int)
     g = wtable.geometry(wtable.NSIDE, wtable.N_MAX, wtable.N_TAU, pix)
@@ -506,11 +507,33 @@ def w_build_leg(args, local):
     W, ms = ctx.w_build(s_nodes, wtable.N_MAX, g, sc)
     per_px = ms[0] / pix.size
     q = 243 * 123
-    fma = 53 * q * float(sc.shape[1])
+    fma = s_nodes.size * q * float(sc.shape[1])
+    # the FP64 denominator: cuBLAS DGEMM 8192^3, best of 5
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda:%d" % local)
+    b = torch.randn_like(a)
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    dgemm_tf = 2 * 8192.0 ** 3 / (best * 1e-3) / 1e12
+    del a, b
+    torch.cuda.empty_cache()
+    tiles = 0
+    for m in range(wtable.N_MAX + 1):
+        L = wtable.N_MAX - m + 1
+        for x0 in range(0, L, 8):
+            tiles += len(range(0, L - x0, 16))
+    exec_tf = 2.0 * tiles * 64 * 128 * q / (per_px * 1e-3) / 1e12
     out = {"pixels_run": int(pix.size), "ms_per_pixel": per_px, "projected_build_s": per_px * 1e-3 * npix,
            "reference_published_s": 7.1 * 3600, "reference_published": "7.1 h for the 53 nodes on one GPU (build_w.py:5-6)",
-           "fp64_fma_per_pixel": fma, "fp64_tflops": 2 * fma / (per_px * 1e-3) / 1e12, "ms_with_copies": ms[1],
-           "finite": bool(np.isfinite(W).all())}
+           "nodes": int(s_nodes.size), "fp64_fma_per_pixel": fma, "fp64_tflops_useful": 2 * fma / (per_px * 1e-3) / 1e12,
+           "fp64_tflops_executed": exec_tf, "dgemm_tflops_measured": dgemm_tf,
+           "frac_of_dgemm": exec_tf / dgemm_tf, "ms_with_copies": ms[1], "finite": bool(np.isfinite(W).all())}
     if not args.no_cpu:
         th, ph = wtable.pix2ang(wtable.NSIDE, pix[:1])
         psi, cg, wq = wtable.quadrature(wtable.N_MAX)
@@ -736,6 +759,9 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--only", choices=("all", "tables"), default="all",
+                    help="'tables': only the offline table-build legs (no analysis, no JSON contract line)")
+    ap.add_argument("--w-nodes", type=int, default=53, help="nodes of the stage-1 table-build leg")
     ap.add_argument("--w-pixels", type=int, default=4, help="sky pixels of the stage-1 table-build leg (0: none)")
     ap.add_argument("--table-build", type=int, default=1, help="run the table-build (stage 3) leg (0: no)")
     ap.add_argument("--io-nodes", type=int, default=8, help="node files of the store-loading leg (0: none)")
@@ -750,7 +776,23 @@ def main():
         raise SystemExit("--warmup must be >= 3")
     if args.impl == "reference":
         return run_reference(args)
+    if args.only == "tables":
+        return run_tables(args)
     return run_b200(args)
+
+
+def run_tables(args):
+    """the offline table-build legs alone (one GPU, rank 0), one JSON line: for profiling those kernels"""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    line = {"legs": "tables"}
+    if args.table_build:
+        line["table_build"] = table_build_leg(args, local)
+    if args.w_pixels > 0:
+        line["w_build"] = w_build_leg(args, local)
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 if __name__ == "__main__":
