@@ -13,7 +13,8 @@
 //   k_w_gemm: for a phase class m the keys form the triangle pw1 = m + 2x, pw2 = m + 2y, x + y <= n_max - m.
 //             A block takes a tile of 8 x-values by 16 y-values (128 keys) and every node (64 rows): a
 //             register-tiled float64 GEMM over q in steps of 16, A[j][q] = Bw_j(q) cos(m dph_q) and
-//             B[q][(x, y)] = m1_q^pw1 m2_q^pw2 formed in shared memory from the 8 + 16 ladder rows of the tile.
+//             B[q][(x, y)] = m1_q^pw1 m2_q^pw2 formed in shared memory from the 8 + 16 ladder rows of the tile;
+//             the next step's inputs arrive by asynchronous copies (two stages) while a step computes.
 //   k_w_scale: W = Wraw * scale, rounded to float32, non-finite entries counted.
 #include <vector>
 
@@ -66,58 +67,84 @@ __global__ void __launch_bounds__(128) k_w_prep(const float *__restrict__ resp, 
         bw[(size_t)j * Q + q] = __dmul_rn(exp(-__dadd_rn(__dmul_rn(s[j], S1), __dmul_rn(s[j], S2))), w);
 }
 
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid)
+{
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(gmem), "r"(valid ? 8 : 0));
+}
+
 __global__ void __launch_bounds__(kWThreads, 2) k_w_gemm(const int4 *__restrict__ tiles, int Q, int n_nodes, int n_max,
                                                          const double *__restrict__ lad1, const double *__restrict__ lad2,
                                                          const double *__restrict__ dph, const double *__restrict__ bw,
                                                          int t0, double w0, double w1, int n_tau, long long n_keys,
                                                          double *__restrict__ Wraw)
 {
-    __shared__ double As[kWQ][kWRows + 1];
+    // two stages of raw inputs filled by asynchronous copies (the next step's while this one computes)
+    __shared__ double Ar[2][kWQ][kWRows + 1];       // damping rows, then times cos(m dph) in place
+    __shared__ double Ld[2][kWX + kWY][kWQ];        // the tile's |R1| and |R2| ladder rows
+    __shared__ double Dp[2][kWQ];
     __shared__ double Bs[kWQ][kWCols + 1];
-    __shared__ double L1s[kWX][kWQ], L2s[kWY][kWQ];
     __shared__ double cm[kWQ];
     const int4 tl = tiles[blockIdx.x];
     const int m = tl.x, x0 = tl.y, y0 = tl.z;
     const int L = n_max - m + 1;
     const int tid = threadIdx.x, tr = tid >> 4, tc = tid & 15;
+    const int nsteps = (Q + kWQ - 1) / kWQ;
+    auto issue = [&](int step, int buf) {
+        const int q0 = step * kWQ;
+        for (int i = tid; i < kWRows * kWQ; i += kWThreads) {
+            const int row = i >> 4, qq = i & 15, q = q0 + qq;
+            const bool ok = row < n_nodes && q < Q;
+            cp_async8(&Ar[buf][qq][row], ok ? bw + (size_t)row * Q + q : bw, ok);
+        }
+        if (tid < kWQ) {
+            const int q = q0 + tid;
+            cp_async8(&Dp[buf][tid], q < Q ? dph + q : dph, q < Q);
+        } else if (tid < kWQ + (kWX + kWY) * kWQ / 4) {
+            for (int i = (tid - kWQ) * 4; i < (tid - kWQ) * 4 + 4; ++i) {
+                const int row = i / kWQ, qq = i - row * kWQ, q = q0 + qq;
+                if (row < kWX) {
+                    const int x = x0 + row;
+                    const bool ok = x <= L - 1 && q < Q;
+                    cp_async8(&Ld[buf][row][qq], ok ? lad1 + (size_t)(m + 2 * x) * Q + q : lad1, ok);
+                } else {
+                    const int y = y0 + row - kWX;
+                    const bool ok = y <= L - 1 && q < Q;
+                    cp_async8(&Ld[buf][row][qq], ok ? lad2 + (size_t)(m + 2 * y) * Q + q : lad2, ok);
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
     double acc[8][8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
 #pragma unroll
         for (int c = 0; c < 8; ++c) acc[r][c] = 0.0;
-    for (int q0 = 0; q0 < Q; q0 += kWQ) {
-        if (tid < kWQ) {
-            const int q = q0 + tid;
-            cm[tid] = q < Q ? cos(__dmul_rn((double)m, dph[q])) : 0.0;
-        } else if (tid < kWQ + (kWX + kWY) * kWQ / 4) {
-            // the tile's ladder rows: 24 rows x 16 points, 4 per thread
-            for (int i = (tid - kWQ) * 4; i < (tid - kWQ) * 4 + 4; ++i) {
-                const int row = i / kWQ, qq = i - row * kWQ, q = q0 + qq;
-                if (row < kWX) {
-                    const int x = x0 + row;
-                    L1s[row][qq] = (x <= L - 1 && q < Q) ? lad1[(size_t)(m + 2 * x) * Q + q] : 0.0;
-                } else {
-                    const int y = y0 + row - kWX;
-                    L2s[row - kWX][qq] = (y <= L - 1 && q < Q) ? lad2[(size_t)(m + 2 * y) * Q + q] : 0.0;
-                }
-            }
-        }
+    issue(0, 0);
+    for (int k = 0; k < nsteps; ++k) {
+        const int buf = k & 1;
+        if (k + 1 < nsteps) issue(k + 1, buf ^ 1);
+        else asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 1;\n" ::);
+        __syncthreads();
+        if (tid < kWQ) cm[tid] = (k * kWQ + tid < Q) ? cos(__dmul_rn((double)m, Dp[buf][tid])) : 0.0;
         __syncthreads();
         for (int i = tid; i < kWRows * kWQ; i += kWThreads) {
-            const int row = i >> 4, qq = i & 15, q = q0 + qq;
-            As[qq][row] = (row < n_nodes && q < Q) ? __dmul_rn(bw[(size_t)row * Q + q], cm[qq]) : 0.0;
+            const int row = i >> 4, qq = i & 15;
+            Ar[buf][qq][row] = __dmul_rn(Ar[buf][qq][row], cm[qq]);
         }
         for (int i = tid; i < kWCols * kWQ; i += kWThreads) {
             const int c = i >> 4, qq = i & 15;
             const int x = c >> 4, y = c & 15;   // column c = y + 16 x
-            Bs[qq][c] = __dmul_rn(L1s[x][qq], L2s[y][qq]);
+            Bs[qq][c] = __dmul_rn(Ld[buf][x][qq], Ld[buf][kWX + y][qq]);
         }
         __syncthreads();
 #pragma unroll 4
         for (int qq = 0; qq < kWQ; ++qq) {
             double a[8], b[8];
 #pragma unroll
-            for (int r = 0; r < 8; ++r) a[r] = As[qq][tr + 8 * r];
+            for (int r = 0; r < 8; ++r) a[r] = Ar[buf][qq][tr + 8 * r];
 #pragma unroll
             for (int c = 0; c < 8; ++c) b[c] = Bs[qq][tc + 16 * c];
 #pragma unroll
@@ -127,6 +154,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_w_gemm(const int4 *__restrict_
         }
         __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
     // thread (tr, tc) holds rows tr + 8 r and columns tc + 16 c: x = x0 + c, y = y0 + tc
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
