@@ -25,7 +25,7 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build")
+           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -81,6 +81,7 @@ def load():
         "exm_store_set_shard": ([P, D], I),
         "exm_bd_build": ([P, I, I, I, I, P, P, P, I, P, I, P, P, P, P], I),
         "exm_w_build": ([P, I, P, I, I, I, P, P, P, P, P, I, P, P, P, I, P, P, P, P], I),
+        "exm_k_edges": ([P, I, I, P, P, I, P, P, I, P, P, P, P], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -242,6 +243,24 @@ class Context:
         self._check(self.lib.exm_bd_build(self.h, nord, ntau, nq, nphif, _p(col), _p(row), _p(lnq), beta.size, _p(beta),
                                           lad.size, _p(lad), _p(T), ctypes.byref(bad), _p(ms)))
         return T, int(bad.value), (float(ms[0]), float(ms[1]))
+
+    def k_edges(self, n_max, Wd, coeff, lnq, gmo, cosm):
+        """stage 2 on the boundary of the (q1, q2) grid: (col, row) float32 (n_max+1, n_tau, nq, nphif) and
+        the kernel milliseconds"""
+        Wd = np.ascontiguousarray(Wd, np.float64)
+        n_keys, n_tau = Wd.shape
+        if n_keys != (n_max + 1) * (n_max + 2) * (n_max + 3) // 6:
+            raise ValueError("Wd must hold every key (n, a, b <= a) of orders 0..n_max")
+        coeff, lnq, gmo, cosm = (np.ascontiguousarray(x, np.float64) for x in (coeff, lnq, gmo, cosm))
+        if coeff.size != n_keys or gmo.size != n_max + 1 or cosm.shape[0] != n_max + 1:
+            raise ValueError("one coefficient per key, one offset and one cosine row per order")
+        nq, nphif = lnq.size, cosm.shape[1]
+        col = np.empty((n_max + 1, n_tau, nq, nphif), np.float32)
+        row = np.empty_like(col)
+        ms = np.zeros(1)
+        self._check(self.lib.exm_k_edges(self.h, n_max, n_tau, _p(Wd), _p(coeff), nq, _p(lnq), _p(gmo), nphif, _p(cosm),
+                                         _p(col), _p(row), _p(ms)))
+        return col, row, float(ms[0])
 
     def w_build(self, s_nodes, n_max, g, scale):
         """stage 1 of the table build over the pixels of geometry g (exmarg_b200.wtable.geometry): W

@@ -11,6 +11,8 @@
 // thread takes (beta, Delta) outputs: the maximum over the orders up to each truncation order, then
 // the sum of exp(E - max) in order of n, in float64 with the products and sums rounded one by one
 // as numpy evaluates them (no fused multiply-add), rounded to float32 at the end.
+#include <vector>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -74,7 +76,170 @@ __global__ void __launch_bounds__(256) k_bd_lse(const float *__restrict__ col, c
     if (bad) atomicAdd(nonfinite, bad);
 }
 
+// Stage 2 on the boundary only (scripts/build_tables/build_k.py:59-82 restricted to q2 = q_last, the
+// column, and q1 = q_last, the row, which is all stage 3 reads): for order n and phase class m = a - b,
+//   C_m(tau, qb) = sum_{a - b = m} c_ab W_ab(tau) exp((a + b) lq1 + (2n - a - b) lq2 - 2n lq_last)
+// with c_ab = C(n, a) C(n, b) (2 if m > 0), qb running over the column (lq1 = lnq[qb], lq2 = lq_last) then
+// the row (lq1 = lq_last, lq2 = lnq[qb - nq], qb - nq < nq - 1).  One block per (n, m, 8 lags); the
+// exponentials of 16 rows at a time in shared memory; each thread holds at most 8 of the block's
+// 8 x (2 nq - 1) outputs.
+constexpr int kKTau = 8;
+constexpr int kKRows = 16;
+
+__global__ void __launch_bounds__(256) k_k_class(const double *__restrict__ Wd, const double *__restrict__ coeff,
+                                                 const int2 *__restrict__ cls, int n_tau, int nq,
+                                                 const double *__restrict__ lnq, double *__restrict__ C)
+{
+    const int nqb = 2 * nq - 1;
+    const int ntc = (n_tau + kKTau - 1) / kKTau;
+    const int c = blockIdx.x / ntc, t0 = (blockIdx.x - c * ntc) * kKTau;
+    const int2 nm = cls[c];   // (n, m)
+    const int n = nm.x, m = nm.y, nrows = n - m + 1;
+    const long long key0 = (long long)n * (n + 1) * (n + 2) / 6;
+    __shared__ double P[kKRows][2 * 128];   // nq <= 128
+    __shared__ double Wm[kKRows][kKTau];
+    const double lql = lnq[nq - 1];
+    const double g = __dmul_rn(2.0 * (double)n, lql);
+    const int nout = kKTau * nqb;   // <= 8 * 256
+    double acc[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+    for (int r0 = 0; r0 < nrows; r0 += kKRows) {
+        const int rn = min(kKRows, nrows - r0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < rn * nqb; i += blockDim.x) {
+            const int r = i / nqb, qb = i - r * nqb;
+            const int a = m + r0 + r, b = a - m;
+            const double lq1 = qb < nq ? lnq[qb] : lql, lq2 = qb < nq ? lql : lnq[qb - nq];
+            const double e = __dsub_rn(__dadd_rn(__dmul_rn((double)(a + b), lq1), __dmul_rn((double)(2 * n - a - b), lq2)), g);
+            P[r][qb] = exp(e);
+        }
+        for (int i = threadIdx.x; i < rn * kKTau; i += blockDim.x) {
+            const int r = i / kKTau, tt = i - r * kKTau, t = t0 + tt;
+            const int a = m + r0 + r, b = a - m;
+            const long long key = key0 + (long long)a * (a + 1) / 2 + b;
+            Wm[r][tt] = t < n_tau ? __dmul_rn(coeff[key], Wd[key * n_tau + t]) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int o = threadIdx.x + k * 256;
+            if (o < nout) {
+                const int tt = o / nqb, qb = o - tt * nqb;
+                double v = acc[k];
+                for (int r = 0; r < rn; ++r) v = fma(Wm[r][tt], P[r][qb], v);
+                acc[k] = v;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int o = threadIdx.x + k * 256;
+        if (o < nout) {
+            const int tt = o / nqb, qb = o - tt * nqb, t = t0 + tt;
+            if (t < n_tau) C[((long long)c * n_tau + t) * nqb + qb] = acc[k];
+        }
+    }
+}
+
+// K_n(tau, qb, phi) = sum_m cos(m phi) C_m(tau, qb); lnK = float32(log(max(K_n, 1e-300)) + (2n lq_last - o_n))
+// into the column col[n][tau][q1][phi] and the row row[n][tau][q2][phi] (the corner q1 = q2 = q_last in both)
+__global__ void __launch_bounds__(256) k_k_phase(const double *__restrict__ C, const int *__restrict__ cls0, int n_tau,
+                                                 int nq, int nphif, const double *__restrict__ cosm, int ncos,
+                                                 const double *__restrict__ gmo, float *__restrict__ col,
+                                                 float *__restrict__ row)
+{
+    const int nqb = 2 * nq - 1;
+    const int n = blockIdx.x / n_tau, t = blockIdx.x - n * n_tau;
+    const int c0 = cls0[n];   // class index of (n, 0); the classes of n are c0 .. c0 + n
+    for (int o = threadIdx.x; o < nqb * nphif; o += blockDim.x) {
+        const int qb = o / nphif, p = o - qb * nphif;
+        double K = 0.0;
+        for (int m = 0; m <= n; ++m)
+            K = fma(cosm[(long long)m * ncos + p], C[((long long)(c0 + m) * n_tau + t) * nqb + qb], K);
+        const float v = (float)__dadd_rn(log(fmax(K, 1e-300)), gmo[n]);
+        const long long base = ((long long)n * n_tau + t) * nq;
+        if (qb < nq) {
+            col[(base + qb) * nphif + p] = v;
+            if (qb == nq - 1) row[(base + qb) * nphif + p] = v;
+        } else {
+            row[(base + qb - nq) * nphif + p] = v;
+        }
+    }
+}
+
 }   // namespace
+
+extern "C" int exm_k_edges(exm_ctx *ctx, int n_max, int n_tau, const double *Wd, const double *coeff, int nq,
+                           const double *lnq, const double *gmo, int nphif, const double *cosm, float *col_out,
+                           float *row_out, double *ms_out)
+{
+    if (!ctx) return EXM_ERR_ARG;
+    try {
+        EXM_CUDA(cudaSetDevice(ctx->dev));
+        if (!(n_max >= 0 && n_max <= 255 && n_tau >= 1 && nq >= 2 && nq <= 128 && nphif >= 1))
+            EXM_THROW(EXM_ERR_ARG, "need 0 <= n_max <= 255, lags >= 1, 2 <= nq <= 128, phases >= 1");
+        if (!(Wd && coeff && lnq && gmo && cosm && col_out && row_out)) EXM_THROW(EXM_ERR_ARG, "null argument");
+        const long long n_keys = (long long)(n_max + 1) * (n_max + 2) * (n_max + 3) / 6;
+        std::vector<int2> cls;
+        std::vector<int> cls0(n_max + 1);
+        for (int n = 0; n <= n_max; ++n) {
+            cls0[n] = (int)cls.size();
+            for (int m = 0; m <= n; ++m) cls.push_back(make_int2(n, m));
+        }
+        const int nqb = 2 * nq - 1;
+        const size_t nC = cls.size() * (size_t)n_tau * nqb, nE = (size_t)(n_max + 1) * n_tau * nq * nphif;
+        dbuf dW, dco, dlnq, dgmo, dcos, dcls, dcls0, dC, dcol, drow;
+        struct Guard {
+            exm_ctx *c;
+            std::vector<dbuf *> b;
+            ~Guard()
+            {
+                for (dbuf *x : b)
+                    if (x->p) exm_free(c, *x);
+            }
+        } guard{ctx, {&dW, &dco, &dlnq, &dgmo, &dcos, &dcls, &dcls0, &dC, &dcol, &drow}};
+        auto up = [&](dbuf &b, const void *src, size_t bytes) {
+            exm_alloc(ctx, b, bytes);
+            EXM_CUDA(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        };
+        cudaEvent_t e0, e1;
+        EXM_CUDA(cudaEventCreate(&e0));
+        EXM_CUDA(cudaEventCreate(&e1));
+        up(dW, Wd, (size_t)n_keys * n_tau * sizeof(double));
+        up(dco, coeff, (size_t)n_keys * sizeof(double));
+        up(dlnq, lnq, nq * sizeof(double));
+        up(dgmo, gmo, (n_max + 1) * sizeof(double));
+        up(dcos, cosm, (size_t)(n_max + 1) * nphif * sizeof(double));
+        up(dcls, cls.data(), cls.size() * sizeof(int2));
+        up(dcls0, cls0.data(), cls0.size() * sizeof(int));
+        exm_alloc(ctx, dC, nC * sizeof(double));
+        exm_alloc(ctx, dcol, nE * sizeof(float));
+        exm_alloc(ctx, drow, nE * sizeof(float));
+        EXM_CUDA(cudaEventRecord(e0, ctx->stream));
+        const long long nblk = (long long)cls.size() * ((n_tau + kKTau - 1) / kKTau);
+        k_k_class<<<(int)nblk, 256, 0, ctx->stream>>>((const double *)dW.p, (const double *)dco.p, (const int2 *)dcls.p,
+                                                      n_tau, nq, (const double *)dlnq.p, (double *)dC.p);
+        k_k_phase<<<(n_max + 1) * n_tau, 256, 0, ctx->stream>>>((const double *)dC.p, (const int *)dcls0.p, n_tau, nq,
+                                                                nphif, (const double *)dcos.p, nphif,
+                                                                (const double *)dgmo.p, (float *)dcol.p, (float *)drow.p);
+        EXM_CUDA(cudaGetLastError());
+        EXM_CUDA(cudaEventRecord(e1, ctx->stream));
+        EXM_CUDA(cudaMemcpyAsync(col_out, dcol.p, nE * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        EXM_CUDA(cudaMemcpyAsync(row_out, drow.p, nE * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+        float k_ms = 0.f;
+        cudaEventElapsedTime(&k_ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (ms_out) ms_out[0] = k_ms;
+        ctx->launches += 2;
+    } catch (const exm_error &e) {
+        ctx->err = e.msg;
+        return e.code;
+    }
+    return 0;
+}
 
 extern "C" int exm_bd_build(exm_ctx *ctx, int nord, int ntau, int nq, int nphif, const float *col, const float *row,
                             const double *lnq, int nb, const double *beta, int n_ladder, const int *ladder,

@@ -1,6 +1,10 @@
-"""The offline table build, stage 3 (the contract of scripts/build_tables/build_bd.py): from stage 2's
-lnK_n(tau, q1, q2, phi) of one node to its table T[tau, phi+, beta, Delta] (the bd_*.npz that
-load_redshift_store reads), on the B200.
+"""The offline table build, stages 2 and 3 (the contracts of scripts/build_tables/build_k.py and
+build_bd.py): from a node's GORFs W (stage 1) through lnK_n(tau, q1, q2, phi) to its table
+T[tau, phi+, beta, Delta] (the bd_*.npz that load_redshift_store reads), on the B200.
+
+build_node_from_w goes from W to the table without the 49 GB lnK of stage 2: the table needs lnK only on
+the last column and last row of the (q1, q2) grid, and exm_k_edges computes just those (with the
+reference's grouping: per phase class m the sum over its (a, b), then the cosine sum over m).
 
 Only the last column and the last row of each (q1, q2) block of lnK enter the table (every order is
 homogeneous in (q1, q2)), so build_node reads just those slices of the memory-mapped lnK and
@@ -54,6 +58,78 @@ def bd_tables(col, row, lnq, ladder=None, device=0, ctx=None):
     if bad:
         raise FloatingPointError("table has non-finite entries at n_max=%d" % ladder[0])
     return {nm: T[i] for i, nm in enumerate(ladder)}, beta, delta, {"kernel_ms": ms[0], "ms": ms[1]}
+
+
+# the data delay grid of stage 2 (build_k.py:31-34): T = 4 s at f_max = 512 Hz, step 1 / (8 f_max)
+K_T, K_FMAX = 4.0, 512.0
+K_QMAX, K_QSPAN, K_NQ, K_NPHI = 100.0, 2000.0, 110, 96
+
+
+def rebin(tau_fine, W_fine, tau_new):
+    """W (keys, fine delays) summed into the bins of tau_new, each fine delay to the nearest new delay
+    (bin edges half-way, the end bins open); sums kept exactly (exmarg/tables.py:253-268)"""
+    order = np.argsort(tau_new)
+    ts = np.asarray(tau_new, np.float64)[order]
+    edges = np.concatenate([[ts[0] - 0.5 * (ts[1] - ts[0])], 0.5 * (ts[1:] + ts[:-1]), [ts[-1] + 0.5 * (ts[-1] - ts[-2])]])
+    idx = np.clip(np.searchsorted(edges, tau_fine) - 1, 0, ts.size - 1)
+    W_fine = np.asarray(W_fine, np.float64)
+    acc = np.zeros((W_fine.shape[0], ts.size))
+    for f in range(W_fine.shape[1]):             # in order of the fine delays, as the reference accumulates
+        acc[:, idx[f]] += W_fine[:, f]
+    out = np.empty_like(acc)
+    out[:, order] = acc
+    return out
+
+
+def load_w_node(stem, T=K_T, fmax=K_FMAX):
+    """a stage-1 node (<stem>.W.npy, .meta.npz) on the data delays: keys (n, a, b <= a), W (keys, lags),
+    tau_idx (build_k.py:37-49)"""
+    m = np.load(stem + ".meta.npz")
+    Wa = np.load(stem + ".W.npy").astype(np.float64)
+    tau_f = m["tau"]
+    n_time = 8 * int(fmax * T)
+    tau_all = np.fft.fftfreq(n_time) * T
+    t_step = T / n_time
+    keep = np.abs(tau_all) <= 1.05 * np.abs(tau_f).max()
+    tau_idx = np.rint(tau_all[keep] / t_step).astype(int)
+    keys = np.asarray(m["keys"]).astype(np.int64)
+    Wd = rebin(tau_f, Wa, tau_all[keep])
+    order = np.lexsort((keys[:, 2], keys[:, 1], keys[:, 0]))
+    return keys[order], Wd[order], tau_idx, float(m["s_node"]), int(m["n_max"])
+
+
+def k_inputs(keys, s, n_max, lnq, nphi=K_NPHI):
+    """coeff per key C(n,a) C(n,b) (x2 for a > b), gmo per order 2n ln q_last - ln(n! s^n), cos(m phi_p) on the
+    first nphi/2 + 1 phases (build_k.py:59-82)"""
+    from scipy.special import comb, gammaln
+    n, a, b = keys[:, 0], keys[:, 1], keys[:, 2]
+    coeff = comb(n, a) * comb(n, b) * np.where(a != b, 2.0, 1.0)
+    orders = np.arange(n_max + 1, dtype=np.float64)
+    gmo = 2.0 * orders * lnq[-1] - (gammaln(orders + 1.0) + orders * np.log(s))
+    phi_g = np.arange(nphi) * (2 * np.pi / nphi)
+    cosm = np.cos(np.outer(np.arange(n_max + 1), phi_g))[:, :nphi // 2 + 1]
+    return coeff, gmo, cosm
+
+
+def build_node_from_w(stem_w, base, nq=K_NQ, nphi=K_NPHI, ladder=None, device=0, ctx=None):
+    """stages 2 and 3 for one node: <stem_w>.W.npy / .meta.npz (build_w.py's output) -> <base>/bd_n<n_max>_s<s>.npz
+    (and the truncated tables of ladder next to it), with only the lnK edges formed; returns the files written"""
+    keys, Wd, tau_idx, s, n_max = load_w_node(stem_w)
+    lnq = np.log(np.geomspace(K_QMAX / K_QSPAN, K_QMAX, nq))
+    coeff, gmo, cosm = k_inputs(keys, s, n_max, lnq, nphi)
+    ctx = ctx or _lib.context(device)
+    col, row, _ = ctx.k_edges(n_max, Wd, coeff, lnq, gmo, cosm)
+    ladder = [n_max] if ladder is None else [int(v) for v in ladder]
+    Ts, beta, delta, _ = bd_tables(col, row, lnq, ladder, ctx=ctx)
+    files = []
+    for nm in ladder:
+        d = out_dir(base, nm, n_max)
+        os.makedirs(d, exist_ok=True)
+        f = os.path.join(d, "bd_n%03d_s%09.3f.npz" % (nm, s))
+        np.savez(f, T=Ts[nm], beta=beta, delta=delta, tau_idx=tau_idx, lnq=lnq, alpha=ALPHA, s_node=s, u_node=s,
+                 n_max=nm, nphif=col.shape[3], norm="taylor_off1")
+        files.append(f)
+    return files
 
 
 def out_dir(base, nmax, nmax_full):

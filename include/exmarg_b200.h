@@ -154,6 +154,19 @@ EXM_API int exm_store_get_node(exm_ctx *ctx, int k, float *T_out);
 
 /* ------------------------------------------------------------------ table build */
 
+/* Stage 2 of the offline table build (scripts/build_tables/build_k.py:59-82) on the last column and
+ * last row of the (q1, q2) grid only -- all that stage 3 reads -- for every order n <= n_max:
+ *   lnK_n(tau, q, phi) = float32(log(max(K_n, 1e-300)) + gmo[n]),
+ *   K_n = sum_m cosm[m][phi] sum_{a - b = m} coeff[key] Wd[key][tau] exp((a+b) lq1 + (2n-a-b) lq2 - 2n lq_last)
+ * with (lq1, lq2) = (lnq[q], lnq[nq-1]) for the column and (lnq[nq-1], lnq[q]) for the row.
+ * Wd (n_keys, n_tau): the node's W rebinned onto the data delays, keys (n, a, b <= a) in order;
+ * coeff (n_keys): C(n,a) C(n,b) (2 when a > b); gmo (n_max+1): 2n lnq[nq-1] - ln(n! s^n);
+ * cosm (n_max+1, nphif): cos(m phi_p).  col_out, row_out: float32 (n_max+1, n_tau, nq, nphif), the
+ * inputs of exm_bd_build.  ms_out (may be NULL): kernel milliseconds.  No 49 GB lnK is formed. */
+EXM_API int exm_k_edges(exm_ctx *ctx, int n_max, int n_tau, const double *Wd, const double *coeff, int nq,
+                        const double *lnq, const double *gmo, int nphif, const double *cosm, float *col_out,
+                        float *row_out, double *ms_out);
+
 /* Stage 3 of the offline table build (scripts/build_tables/build_bd.py:53-77): one node's table
  * T[tau, phi, beta, Delta] = log sum_{n <= n_max} exp(n beta + g_n(Delta)), float64 arithmetic,
  * float32 result, for each truncation order n_max in ladder (n_ladder of them).

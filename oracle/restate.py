@@ -506,3 +506,42 @@ def w_table_s(s_nodes, n_max, nside, n_tau, pix2ang, rounding="numpy"):
     scale = np.exp(np.minimum(n_key[None, :] * np.log(s)[:, None] - gammaln(n_key + 1.0)[None, :]
                               + n_key[None, :] * np.log(2.0), 700.0))
     return tau, Wraw * scale[:, None, :]
+
+
+# ----------------------------------------------------------------------------- table build, stage 2
+
+def k_order(n, s, keys, Wd, lnq, phi, pairs=None):
+    """scripts/build_tables/build_k.py:59-82 for one order n: lnK_n (n_tau, n_pairs, n_phi) float32 on the
+    (q1, q2) pairs given as index arrays (q1, q2) (default: the whole nq x nq grid, row-major), with the
+    reference's grouping: per phase class m = a - b the sum over its (a, b) as one product of matrices, then
+    the cosine sum over m."""
+    from scipy.special import comb, gammaln
+    nq = lnq.size
+    if pairs is None:
+        q1, q2 = (x.ravel() for x in np.meshgrid(np.arange(nq), np.arange(nq), indexing="ij"))
+    else:
+        q1, q2 = pairs
+    l1, l2 = lnq[q1], lnq[q2]
+    o_n = gammaln(n + 1.0) + n * np.log(s)
+    g = 2.0 * n * np.maximum(l1, l2)
+    rows = [(j, int(a), int(b)) for j, (nn, a, b) in enumerate(keys) if nn == n]
+    ms = sorted({a - b for _, a, b in rows})
+    C = np.empty((len(ms), Wd.shape[1] * l1.size))
+    for i, m in enumerate(ms):
+        sel = [(j, a, b) for j, a, b in rows if a - b == m]
+        Wm = np.array([comb(n, a) * comb(n, b) * (2.0 if m else 1.0) * Wd[j] for j, a, b in sel])
+        P = np.exp(np.stack([(a + b) * l1 + (2 * n - a - b) * l2 - g for _, a, b in sel]))
+        C[i] = (Wm.T @ P).ravel()
+    K = (C.T @ np.cos(np.outer(ms, phi))).reshape(Wd.shape[1], l1.size, phi.size)
+    return (np.log(np.maximum(K, 1e-300)) + (g - o_n)[None, :, None]).astype(np.float32)
+
+
+def k_edges(keys, Wd, s, n_max, lnq, nphi):
+    """lnK's last column (q2 = q_last) and last row (q1 = q_last), (orders, lags, nq, nphi/2 + 1) float32 each"""
+    nq = lnq.size
+    phi = (np.arange(nphi) * (2 * np.pi / nphi))[:nphi // 2 + 1]
+    last = np.full(nq, nq - 1)
+    ar = np.arange(nq)
+    col = np.stack([k_order(n, s, keys, Wd, lnq, phi, (ar, last)) for n in range(n_max + 1)]).transpose(0, 1, 2, 3)
+    row = np.stack([k_order(n, s, keys, Wd, lnq, phi, (last, ar)) for n in range(n_max + 1)])
+    return col, row

@@ -1,6 +1,6 @@
 """Golden vectors for the pe_intrinsic path, produced by running the REFERENCE's own CPU
-code (exmarg.search: numpy + numba; its table builders scripts/build_tables/build_bd.py and
-w_gpu.py, the latter with numpy standing in for cupy) in a container where its source tree is present.
+code (exmarg.search: numpy + numba; its table builders scripts/build_tables/w_gpu.py, build_k.py and
+build_bd.py, w_gpu.py with numpy standing in for cupy) in a container where its source tree is present.
 
     python tests/golden/make_golden.py [reference src dir [case ...]]
 
@@ -220,6 +220,52 @@ def make_w(name, c, ref_root):
     print(name, out.shape, float(np.abs(out).max()))
 
 
+# stage 2 of the table build on the reference's own stage-1 output: node 1 of w1 written as build_w writes it,
+# the reference's build_k load_node (delay rebin) and compile_order (every order, on a 12-point magnitude
+# grid and 8 phases), then its build_bd on that lnK
+K_CASES = {
+    "k1": dict(w_case="w1", node=1, nq=12, nphi=8),
+}
+
+
+def make_k(name, c, ref_root):
+    import importlib.util
+    import tempfile
+    from exmarg_b200 import wtable
+    z = np.load(os.path.join(HERE, c["w_case"] + ".npz"))
+    n_max, s = int(z["n_max"]), float(z["s"][c["node"]])
+    with tempfile.TemporaryDirectory() as d:
+        stem_w = os.path.join(d, "sladder_n%03d_s%09.3f" % (n_max, s))
+        wtable.save_node(stem_w, s, z["tau"], z["W"][c["node"]], n_max, int(z["nside"]))
+        spec = importlib.util.spec_from_file_location("build_k", os.path.join(ref_root, "scripts", "build_tables",
+                                                                              "build_k.py"))
+        bk = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(bk)
+        bk.NQ, bk.NPHI = c["nq"], c["nphi"]
+        keys, WM, tau_idx = bk.load_node(stem_w)
+        lnq = np.log(np.geomspace(bk.QMAX / bk.QSPAN, bk.QMAX, c["nq"]))
+        phi_g = np.arange(c["nphi"]) * (2 * np.pi / c["nphi"])
+        by_n = {n: [] for n in range(n_max + 1)}
+        for j, (n, a, b) in enumerate(keys):
+            by_n[int(n)].append((j, int(a), int(b)))
+        lnK = np.stack([bk.compile_order(n, s, keys, WM, lnq, by_n, phi_g, tau_idx.size) for n in range(n_max + 1)])
+        stem_k = os.path.join(d, "kstore_n%03d_s%09.3f" % (n_max, s))
+        np.save(stem_k + ".lnK.npy", lnK)
+        np.savez(stem_k + ".meta.npz", s_node=s, lnq=lnq, tau_idx=tau_idx)
+        os.environ["BD_NMAX_LADDER"] = ""
+        spec = importlib.util.spec_from_file_location("build_bd", os.path.join(ref_root, "scripts", "build_tables",
+                                                                              "build_bd.py"))
+        bd = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(bd)
+        base = os.path.join(d, "bd")
+        bd.build_node(stem_k, base)
+        out = np.load(os.path.join(base, "bd_n%03d_s%09.3f.npz" % (n_max, s)))
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), s=s, n_max=n_max, keys=keys, WM=WM, tau_idx=tau_idx,
+                            lnq=lnq, nphi=c["nphi"], lnK=lnK, T=out["T"], beta=out["beta"], delta=out["delta"],
+                            W_tau=z["tau"], W=z["W"][c["node"]])
+    print(name, lnK.shape, WM.shape)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
     only = sys.argv[2:] if len(sys.argv) > 2 else None
@@ -238,6 +284,10 @@ def main():
         if only is None or name in only:
             refimport.import_reference(src)          # exmarg on the path, with its stub modules
             make_w(name, c, os.path.dirname(os.path.abspath(src)))
+    for name, c in K_CASES.items():
+        if only is None or name in only:
+            refimport.import_reference(src)
+            make_k(name, c, os.path.dirname(os.path.abspath(src)))
 
 
 if __name__ == "__main__":
