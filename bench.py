@@ -478,8 +478,25 @@ def table_build_leg(args, local):
     out = {"orders": nord, "lags": ntau, "table": [ntau, nphif, int(beta.size), 2 * nq - 1], "kernel_ms": k_ms,
            "ms_with_copies": all_ms, "non_finite": bad, "exp_per_s": nout * nord / (k_ms * 1e-3),
            "seconds_for_53_nodes": all_ms * 1e-3 * 53}
+    # stage 2 on the lnK edges for the same node shape: synthetic rebinned W of every key (n <= 120) on 87 lags,
+    # the production magnitude grid (110) and 96 phases
+    from exmarg_b200 import wtable
+    keys = np.array(wtable.keys(nord - 1))
+    Wd = np.exp(rng.normal(-3.0, 1.0, (keys.shape[0], ntau)))
+    coeff, gmo, cosm = tables.k_inputs(keys, 25.0, nord - 1, lnq, 96)
+    k_runs = sorted(ctx.k_edges(nord - 1, Wd, coeff, lnq, gmo, cosm)[2] for _ in range(3))
+    out["stage2_edges_kernel_ms"] = k_runs[1]
+    out["stage2_plus_3_kernel_ms"] = k_runs[1] + k_ms
     if not args.no_cpu:
         from oracle import restate
+        phi = np.arange(96) * (2 * np.pi / 96)
+        t0 = time.perf_counter()
+        restate.k_order(60, 25.0, keys, Wd, lnq, phi)
+        one = time.perf_counter() - t0
+        scale = sum((n + 1) ** 2 for n in range(nord)) / 61.0 ** 2
+        out["cpu_baseline_stage2"] = {"seconds_per_node": one * scale, "cores": "numpy BLAS threads", "kind": "port",
+                                      "sample": "order 60 of 121 on the full 110 x 110 x 96 grid (the reference's "
+                                                "work), scaled by sum (n+1)^2 / 61^2"}
         t0 = time.perf_counter()
         ref = restate.bd_tables(col[:, :1], row[:, :1], lnq, beta, [nord - 1])[nord - 1]
         cpu_lag = time.perf_counter() - t0
