@@ -204,7 +204,9 @@ def make_bank(n, seed, mc=(10.0, 40.0), q=(0.25, 1.0), chi=(-0.5, 0.5)):
 
 # ----------------------------------------------------------------------------- tables
 
-S_NODES_PROD = np.geomspace(4000.0 * 10.0 ** -5.39794001, 4000.0, 53)   # the 53 signal-power nodes
+# the 53 signal-power nodes of the published store: logarithmic from s_min to 4000 (data/tables/s_grid.npz:
+# s_min, s_max, n_nodes; equal to its s_nodes within 2.3e-15)
+S_NODES_PROD = np.geomspace(0.004264528739608287, 4000.0, 53)
 ALPHA = np.geomspace(0.16, 4.0e4, 30)                                    # amplitude axis of each node
 
 
