@@ -114,22 +114,26 @@ def k_inputs(keys, s, n_max, lnq, nphi=K_NPHI):
 def build_node_from_w(stem_w, base, nq=K_NQ, nphi=K_NPHI, ladder=None, device=0, ctx=None):
     """stages 2 and 3 for one node: <stem_w>.W.npy / .meta.npz (build_w.py's output) -> <base>/bd_n<n_max>_s<s>.npz
     (and the truncated tables of ladder next to it), with only the lnK edges formed; returns the files written"""
+    meta = np.load(stem_w + ".meta.npz")
+    s, n_max = float(meta["s_node"]), int(meta["n_max"])
+    ladder = [n_max] if ladder is None else [int(v) for v in ladder]
+    if max(ladder) > n_max:
+        raise ValueError("a truncation order exceeds the node's n_max")
+    outs = {nm: os.path.join(out_dir(base, nm, n_max), "bd_n%03d_s%09.3f.npz" % (nm, s)) for nm in ladder}
+    todo = [nm for nm in ladder if not os.path.exists(outs[nm])]   # tables already written are skipped
+    if not todo:
+        return []
     keys, Wd, tau_idx, s, n_max = load_w_node(stem_w)
     lnq = np.log(np.geomspace(K_QMAX / K_QSPAN, K_QMAX, nq))
     coeff, gmo, cosm = k_inputs(keys, s, n_max, lnq, nphi)
     ctx = ctx or _lib.context(device)
     col, row, _ = ctx.k_edges(n_max, Wd, coeff, lnq, gmo, cosm)
-    ladder = [n_max] if ladder is None else [int(v) for v in ladder]
-    Ts, beta, delta, _ = bd_tables(col, row, lnq, ladder, ctx=ctx)
-    files = []
-    for nm in ladder:
-        d = out_dir(base, nm, n_max)
-        os.makedirs(d, exist_ok=True)
-        f = os.path.join(d, "bd_n%03d_s%09.3f.npz" % (nm, s))
-        np.savez(f, T=Ts[nm], beta=beta, delta=delta, tau_idx=tau_idx, lnq=lnq, alpha=ALPHA, s_node=s, u_node=s,
+    Ts, beta, delta, _ = bd_tables(col, row, lnq, todo, ctx=ctx)
+    for nm in todo:
+        os.makedirs(os.path.dirname(outs[nm]), exist_ok=True)
+        np.savez(outs[nm], T=Ts[nm], beta=beta, delta=delta, tau_idx=tau_idx, lnq=lnq, alpha=ALPHA, s_node=s, u_node=s,
                  n_max=nm, nphif=col.shape[3], norm="taylor_off1")
-        files.append(f)
-    return files
+    return [outs[nm] for nm in todo]
 
 
 def out_dir(base, nmax, nmax_full):
@@ -167,3 +171,50 @@ def build_node(stem, base, ladder=None, device=0):
                  u_node=s, n_max=nm, nphif=nphif, norm="taylor_off1")
     print("s=%g done: %d orders %s in %.1f s" % (s, len(todo), todo, time.time() - t0), flush=True)
     return [outs[nm] for nm in todo]
+
+
+def node_stems(directory, prefix, suffix):
+    """the stems <directory>/<prefix>n<order>_s<s> of the files <stem><suffix>, in ascending s"""
+    import glob
+    files = glob.glob(os.path.join(directory, prefix + "n*_s*" + suffix))
+    stems = [f[:-len(suffix)] for f in files]
+    return sorted(stems, key=lambda t: float(os.path.basename(t).split("_s")[-1]))
+
+
+def main(argv=None):
+    """python -m exmarg_b200.tables bd <k_dir> <out_dir> [node indices]     stage 3 from stage 2's lnK (build_bd.py)
+    python -m exmarg_b200.tables from-w <w_dir> <out_dir> [node indices] stages 2 + 3 from stage 1's W
+    Node indices count the input files in ascending s (default: all).  BD_NMAX_LADDER as build_bd.py reads it."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m exmarg_b200.tables", description=main.__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("mode", choices=("bd", "from-w"))
+    ap.add_argument("in_dir")
+    ap.add_argument("out_dir")
+    ap.add_argument("nodes", nargs="*", type=int)
+    ap.add_argument("--nq", type=int, default=K_NQ, help="from-w: magnitude points of stage 2 (build_k.py: 110)")
+    ap.add_argument("--nphi", type=int, default=K_NPHI, help="from-w: phase points of stage 2 (build_k.py: 96)")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+    env = os.environ.get("BD_NMAX_LADDER", "").strip()
+    ladder = [int(v) for v in env.split(",")] if env else None
+    if args.mode == "bd":
+        stems = node_stems(args.in_dir, "kstore_", ".meta.npz")
+    else:
+        stems = node_stems(args.in_dir, "sladder_", ".meta.npz")
+    if not stems:
+        raise SystemExit("no input nodes in %s" % args.in_dir)
+    pick = args.nodes or list(range(len(stems)))
+    for i in pick:
+        if args.mode == "bd":
+            build_node(stems[i], args.out_dir, ladder, args.device)
+        else:
+            t0 = time.time()
+            files = build_node_from_w(stems[i], args.out_dir, nq=args.nq, nphi=args.nphi, ladder=ladder,
+                                      device=args.device)
+            print("%s: %d tables in %.1f s" % (os.path.basename(stems[i]), len(files), time.time() - t0), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -184,3 +184,33 @@ def build_w(out, s_nodes, n_max=N_MAX, nside=NSIDE, n_tau=N_TAU, device=0):
     np.savez(os.path.join(out, "manifest.npz"), s_nodes=np.asarray(s_nodes), n_max=n_max, nside=nside, n_tau=n_tau,
              s_min=float(np.min(s_nodes)), s_max=float(np.max(s_nodes)), built_s=seconds)
     return seconds
+
+
+def main(argv=None):
+    """python -m exmarg_b200.wtable <out_dir> [node indices]   the W tables of the nodes (build_w.py)
+    Nodes: the 53 of the published store (exmarg_b200.synth.S_NODES_PROD), or --s-grid <npz with s_nodes>."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m exmarg_b200.wtable", description=main.__doc__,
+                                 formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("out_dir")
+    ap.add_argument("nodes", nargs="*", type=int)
+    ap.add_argument("--s-grid", default=None)
+    ap.add_argument("--n-max", type=int, default=N_MAX)
+    ap.add_argument("--nside", type=int, default=NSIDE)
+    ap.add_argument("--n-tau", type=int, default=N_TAU)
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+    if args.s_grid:
+        s_all = np.load(args.s_grid)["s_nodes"]
+    else:
+        from .synth import S_NODES_PROD as s_all
+    s_nodes = np.asarray(s_all)[args.nodes or list(range(len(s_all)))]
+    if s_nodes.size > 64:
+        raise SystemExit("at most 64 nodes per build")
+    seconds = build_w(args.out_dir, s_nodes, args.n_max, args.nside, args.n_tau, args.device)
+    print("%d nodes in %.0f s, written to %s" % (s_nodes.size, seconds, args.out_dir), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

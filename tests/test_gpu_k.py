@@ -73,3 +73,17 @@ def test_edges_against_oracle_more_orders():
     rc, rr = restate.k_edges(keys, Wd, s, n_max, lnq, nphi)
     _check_edges(col, rc, gmo)
     _check_edges(row, rr, gmo)
+
+
+def test_cli_from_w(tmp_path):
+    """python -m exmarg_b200.tables from-w on the golden node; a second run finds the table and skips it"""
+    z = np.load(GOLDEN)
+    w_dir = os.path.join(str(tmp_path), "w")
+    os.makedirs(w_dir)
+    stem = os.path.join(w_dir, "sladder_n%03d_s%09.3f" % (int(z["n_max"]), float(z["s"])))
+    wtable.save_node(stem, float(z["s"]), z["W_tau"], z["W"], int(z["n_max"]), 2)
+    out = os.path.join(str(tmp_path), "bd")
+    assert tables.main(["from-w", w_dir, out, "--nq", str(z["lnq"].size), "--nphi", str(int(z["nphi"]))]) == 0
+    f = os.path.join(out, "bd_n%03d_s%09.3f.npz" % (int(z["n_max"]), float(z["s"])))
+    assert ulps(np.load(f)["T"], z["T"]).max() <= 2
+    assert tables.build_node_from_w(stem, out, nq=z["lnq"].size, nphi=int(z["nphi"])) == []

@@ -2,6 +2,8 @@
 its T.npy data (what exm_store_load reads), and upload_store streams a mapped store from its files and
 sends a store read into memory from its host arrays."""
 
+import os
+
 import numpy as np
 import pytest
 
@@ -66,3 +68,13 @@ def test_upload_sends_host_tables(store_dir):
     upload_store(st, ctx)
     assert ctx.load["paths"] is None
     assert all(h is T for h, T in zip(ctx.load["hosts"], st.tables))
+
+
+def test_table_cli_orders_nodes_by_s(tmp_path):
+    from exmarg_b200 import tables
+    for s in (12.5, 0.004, 3.0):
+        open(os.path.join(str(tmp_path), "sladder_n120_s%09.3f.meta.npz" % s), "w").close()
+    open(os.path.join(str(tmp_path), "other.meta.npz"), "w").close()
+    stems = tables.node_stems(str(tmp_path), "sladder_", ".meta.npz")
+    assert [os.path.basename(t) for t in stems] == ["sladder_n120_s00000.004", "sladder_n120_s00003.000",
+                                                   "sladder_n120_s00012.500"]
