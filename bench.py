@@ -579,24 +579,25 @@ def w_build_leg(args, local):
 
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
-    banks -- all 2048 templates on 8 s segments, the first 1024 on 8 s segments, all 2048 on 4 s
-    segments (n_time 16384) -- in equal parts, graph replay on the workers.  'batched': every request
+    banks -- all 2048 templates on 8 s segments, the first 1024 on 16 s segments (n_time 65536), all 2048
+    on 4 s segments (n_time 16384) -- in equal parts, graph replay on the workers.  'batched': every request
     queued at once (segments in flight together); 'poisson': arrivals at 80 % of the plain path's
     2048-template 8 s capacity.  Served ln Lambda of the 2048-template 8 s bank is compared bitwise
     with the plain call's."""
     import exmarg_b200 as eb
     from exmarg_b200 import synth
     from exmarg_b200.serve import Request, Server, latency_stats
-    half = eb.MassBank(rows[:1024, 0], rows[:1024, 1], rows[:1024, 2], seg, "b200", device_index=local)
+    seg16 = synth.make_segments(8, segment_seed(0) + 1616, T=16.0, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
+    long = eb.MassBank(rows[:1024, 0], rows[:1024, 1], rows[:1024, 2], seg16, "b200", device_index=local)
     seg4 = synth.make_segments(8, segment_seed(0) + 777, T=4.0, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
     short = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg4, "b200", device_index=local)
-    banks = {"bank2048": bank, "bank1024": half, "bank2048_4s": short}
-    segs = {"bank2048": seg, "bank1024": seg, "bank2048_4s": seg4}
+    banks = {"bank2048": bank, "bank1024_16s": long, "bank2048_4s": short}
+    segs = {"bank2048": seg, "bank1024_16s": seg16, "bank2048_4s": seg4}
     first = args.warmup
     n_req = args.serve_requests
     n_rows = len(plain)
-    keys = ("bank2048", "bank1024", "bank2048_4s")
-    mix = [(keys[i % 3], first + (i % n_rows) if i % 3 < 2 else i % 8) for i in range(n_req)]
+    keys = ("bank2048", "bank1024_16s", "bank2048_4s")
+    mix = [(keys[i % 3], first + (i % n_rows) if i % 3 == 0 else i % 8) for i in range(n_req)]
     out = {}
     srv = Server(store, banks, device=local, max_workers=args.serve_workers, graph=True)
     try:
@@ -622,7 +623,7 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
                  "service_ms_p50": st["service_ms_p50"], "service_ms_max": st["service_ms_max"],
                  "workers_created": srv.n_created, "workers_evicted": srv.n_evicted,
                  "identical_to_plain": same,
-                 "banks": "2048 templates / 8 s, 1024 / 8 s, 2048 / 4 s segments (1:1:1)"}
+                 "banks": "2048 templates / 8 s, 1024 / 16 s, 2048 / 4 s segments (1:1:1)"}
             if leg == "poisson":
                 d["offered_per_s"] = 0.8 * capacity
             out[leg] = d
