@@ -587,9 +587,12 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     import exmarg_b200 as eb
     from exmarg_b200 import synth
     from exmarg_b200.serve import Request, Server, latency_stats
-    seg16 = synth.make_segments(8, segment_seed(0) + 1616, T=16.0, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
+    # the 16 s and 4 s segments follow the serving config's data: network SNR U(0, 50), 90% noise-only
+    seg16 = synth.make_segments(8, segment_seed(0) + 1616, T=16.0, fmax=FMAX, snr=(0.0, 50.0), noise_only=0.9, mc=25.0,
+                                q=0.8, chi=0.1)
     long = eb.MassBank(rows[:1024, 0], rows[:1024, 1], rows[:1024, 2], seg16, "b200", device_index=local)
-    seg4 = synth.make_segments(8, segment_seed(0) + 777, T=4.0, fmax=FMAX, snr=15.0, mc=25.0, q=0.8, chi=0.1)
+    seg4 = synth.make_segments(8, segment_seed(0) + 777, T=4.0, fmax=FMAX, snr=(0.0, 50.0), noise_only=0.9, mc=25.0,
+                               q=0.8, chi=0.1)
     short = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg4, "b200", device_index=local)
     banks = {"bank2048": bank, "bank1024_16s": long, "bank2048_4s": short}
     segs = {"bank2048": seg, "bank1024_16s": seg16, "bank2048_4s": seg4}
@@ -623,7 +626,7 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
                  "service_ms_p50": st["service_ms_p50"], "service_ms_max": st["service_ms_max"],
                  "workers_created": srv.n_created, "workers_evicted": srv.n_evicted,
                  "identical_to_plain": same,
-                 "banks": "2048 templates / 8 s, 1024 / 16 s, 2048 / 4 s segments (1:1:1)"}
+                 "banks": "2048 templates / 8 s (SNR 15), 1024 / 16 s and 2048 / 4 s (SNR U(0, 50), 90% noise-only)"}
             if leg == "poisson":
                 d["offered_per_s"] = 0.8 * capacity
             out[leg] = d
