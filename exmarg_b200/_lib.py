@@ -141,6 +141,8 @@ class Context:
         self.nm = self.nfreq = self.n_time = None
         self.gather_cfg = None          # the launch shape chosen by autotune or set_gather_cfg (None: default)
         self.gather_chunk_pct = 100     # templates per gather block, percent of the default
+        self.store_shape = None         # (nodes, lags, phase planes, nb, nd, dtype) of the resident store
+        self.device_total = device_memory(device)[1]   # identifies the device model in the autotune cache
 
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
@@ -188,6 +190,7 @@ class Context:
         self._check(self.lib.exm_store_init(self.h, n_nodes, ntau, nphif, nb, nd, dtype, _p(tau), beta0, dbeta,
                                             delta0, ddelta))
         self.store_token = self.prep_token = None
+        self.store_shape = (int(n_nodes), int(ntau), int(nphif), int(nb), int(nd), int(dtype))
 
     def store_set_node(self, k, s, alpha_lo, alpha_hi, T):
         T = np.ascontiguousarray(T, np.float32)

@@ -10,6 +10,9 @@ tables stay resident and the device path sizes its own launches.  With a 'cpu' o
 'gpu' bank the call goes to the reference's exmarg.search.pe_intrinsic.
 """
 
+import json
+import os
+
 import numpy as np
 
 from . import _lib
@@ -59,17 +62,80 @@ def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, 
     seg = read_segments(segments, rows)
     ctx = prepare(bank, store, prior, ymin)
     seeds = seed + np.asarray(seg["rows"], np.int64)
+    apply_tuned(ctx, n_loud, n_random)
     lnl, lnb = ctx.pe_intrinsic(seg["d_H"], seg["d_L"], seg["sig2_H"], seg["sig2_L"], seeds, n_loud, n_random)
     return dict(M=bank.M, q=bank.q, chi=bank.chi, u=bank.u, ln_lambda=lnl, ln_b=lnb, rows=seg["rows"])
 
 
-def autotune(bank, store, segments, prior="volume", ymin=0.1267, n_loud=1024, n_random=1024, reps=2):
+def autotune(bank, store, segments, prior="volume", ymin=0.1267, n_loud=1024, n_random=1024, reps=2, cache=True):
     """choose the plane gather's launch shape and templates per block for this bank and store: analyse
     the first segment once, then time every shape on it (CUDA events), then the block size at 50 / 150 /
-    200% with the best shape; later calls on the context use the fastest.
+    200% with the best shape; later calls on the context use the fastest.  With cache, the choice is
+    also written to the autotune cache (tune_cache_path()), from which later processes take it for the
+    same workload shape on the same device model without tuning.
     returns (chosen shape index, ms per launch: each shape, then each block size)"""
     pe_intrinsic(segments, bank, store, rows=[0], prior=prior, ymin=ymin, n_loud=n_loud, n_random=n_random)
-    return bank.ctx.autotune(n_loud, n_random, reps)
+    ctx = bank.ctx
+    best, ms = ctx.autotune(n_loud, n_random, reps)
+    if cache:
+        record_tuned(ctx, n_loud, n_random, best, ctx.gather_chunk_pct, ms)
+    return best, ms
+
+
+# ----------------------------------------------------------------------------- autotune cache
+
+def tune_cache_path():
+    """EXMARG_B200_TUNE_CACHE, else ~/.cache/exmarg_b200/autotune.json"""
+    p = os.environ.get("EXMARG_B200_TUNE_CACHE")
+    return p if p else os.path.join(os.path.expanduser("~"), ".cache", "exmarg_b200", "autotune.json")
+
+
+def tune_key(ctx, n_loud, n_random):
+    """the workload shape the gather's best launch depends on, and the device model (its memory size)"""
+    nn, ntau, nphif, nb, nd, dtype = ctx.store_shape
+    return "dev%d|templates%d|n_time%d|nodes%d|lags%d|planes%d|nb%d|nd%d|dtype%d|walk%d" % (
+        int(ctx.device_total) >> 30, ctx.nm, ctx.n_time, nn, ntau, nphif, nb, nd, dtype,
+        (n_loud + n_random) if n_loud > 0 else ctx.n_time)
+
+
+def _read_cache(path):
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def record_tuned(ctx, n_loud, n_random, shape, chunk_pct, ms=None):
+    """write an autotune choice to the cache (a JSON object keyed by tune_key; written atomically)"""
+    path = tune_cache_path()
+    d = _read_cache(path)
+    d[tune_key(ctx, n_loud, n_random)] = {"shape": int(shape), "chunk_pct": int(chunk_pct),
+                                          "ms": [float(v) for v in np.asarray(ms if ms is not None else [])[:16]]}
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    tmp = path + ".%d.tmp" % os.getpid()
+    with open(tmp, "w") as fh:
+        json.dump(d, fh, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def apply_tuned(ctx, n_loud, n_random):
+    """use the cached choice for this workload when the context has none of its own (autotune or
+    set_gather_cfg); returns the entry applied or None.  Child contexts keep the launch their parent
+    chose (the library copies it when they are made), so that served and plain results agree bitwise."""
+    if ctx.gather_cfg is not None or getattr(ctx, "parent", None) is not None:
+        return None
+    if ctx.store_shape is None or ctx.nm is None:
+        return None
+    key = tune_key(ctx, n_loud, n_random)
+    if getattr(ctx, "tune_looked_up", None) == key:   # looked up already for this workload: no entry
+        return None
+    ctx.tune_looked_up = key
+    e = _read_cache(tune_cache_path()).get(key)
+    if not e or not 0 <= int(e.get("shape", -1)) < len(_lib.GATHER_SHAPES):
+        return None
+    ctx.set_gather_cfg(int(e["shape"]), int(e.get("chunk_pct", 0)))
+    return e
 
 
 def distance_weights(y, prior, ymin):

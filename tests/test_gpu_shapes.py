@@ -58,3 +58,23 @@ def test_bad_shape_is_rejected():
         ctx.set_gather_cfg(len(_lib.GATHER_SHAPES), 100)
     with pytest.raises(ValueError):
         ctx.set_gather_cfg(0, 5)
+
+
+def test_autotune_cache_reaches_a_new_context(tmp_path, monkeypatch):
+    """autotune(cache=True) records the choice; a fresh context of the same workload takes it without tuning"""
+    monkeypatch.setenv("EXMARG_B200_TUNE_CACHE", str(tmp_path / "autotune.json"))
+    fx = Fixture("config1")
+    kw = dict(prior=fx.prior_arg, ymin=fx.ymin, n_loud=fx.n_loud, n_random=fx.n_random)
+    a, b = _lib.Context(0), _lib.Context(0)
+    try:
+        bank_a = fx.b200_bank()
+        bank_a._ctx = a
+        best, _ = eb.autotune(bank_a, fx.store, fx.seg, reps=1, **kw)
+        bank_b = fx.b200_bank()
+        bank_b._ctx = b
+        res = eb.pe_intrinsic(fx.seg, bank_b, fx.store, **kw)
+        assert b.gather_cfg == best and b.gather_chunk_pct == a.gather_chunk_pct
+        assert np.abs(res["ln_b"] - fx.ln_b).max() <= 1e-5
+    finally:
+        a.close()
+        b.close()
