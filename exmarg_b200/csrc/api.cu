@@ -3,6 +3,7 @@
 // node / distance log-sum-exp -> ln B), plus the stage entry points.
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <numeric>
 
 #include <mutex>
@@ -213,7 +214,8 @@ extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
 {
     if (!out) return EXM_ERR_ARG;
     *out = nullptr;
-    exm_ctx *ctx = new exm_ctx();
+    exm_ctx *ctx = new (std::nothrow) exm_ctx();
+    if (!ctx) return EXM_ERR_OOM;
     try {
         EXM_CUDA(cudaSetDevice(device));
         ctx->dev = device;
@@ -232,6 +234,11 @@ extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return e.code;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "exm_ctx_create: %s\n", e.what());
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return EXM_ERR_OOM;
     }
     *out = ctx;
     return EXM_OK;
@@ -246,7 +253,11 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         parent->err = "the parent context has no complete store to share";
         return EXM_ERR_STATE;
     }
-    exm_ctx *ctx = new exm_ctx();
+    exm_ctx *ctx = new (std::nothrow) exm_ctx();
+    if (!ctx) {
+        parent->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    }
     try {
         EXM_CUDA(cudaSetDevice(parent->dev));
         ctx->dev = parent->dev;
@@ -293,6 +304,12 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
         return e.code;
+    } catch (const std::exception &e) {
+        parent->err = e.what();
+        exm_free(ctx, ctx->d_stats);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return EXM_ERR_OOM;
     }
     ctx->parent = parent;
     parent->n_children.fetch_add(1);

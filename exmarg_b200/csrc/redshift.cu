@@ -207,6 +207,12 @@ extern "C" int exm_redshift_grid(exm_ctx *ctx, int nn1, int nm, const double *yN
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return EXM_OK;
 }
@@ -240,6 +246,12 @@ extern "C" int exm_source_frame(exm_ctx *ctx, const double *lamN, double *ln_lam
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return EXM_OK;
 }

@@ -212,12 +212,17 @@ void exm_store_load_run(exm_ctx *ctx, int first, int n, const char *const *paths
     };
 
     std::vector<std::thread> pool;
-    for (int t = 0; t < nrd; ++t) pool.emplace_back(reader);
     long long wait_ns = 0;
     std::string iss_err;
     int iss_code = 0;
     try {
-        for (int j = 0; j < njobs; ++j) {
+        for (int t = 0; t < nrd; ++t) pool.emplace_back(reader);
+    } catch (const std::exception &e) {   // a reader could not start: stop the ones that did
+        iss_code = EXM_ERR_STATE;
+        iss_err = std::string("store load: cannot start reader threads: ") + e.what();
+    }
+    try {
+        for (int j = 0; j < njobs && iss_code == 0; ++j) {   // (no issue at all when a reader did not start)
             const auto t0 = clk::now();
             {
                 std::unique_lock<std::mutex> lk(mu);
@@ -255,6 +260,12 @@ void exm_store_load_run(exm_ctx *ctx, int first, int n, const char *const *paths
     } catch (const exm_error &e) {
         iss_code = e.code;
         iss_err = e.msg;
+    } catch (const std::bad_alloc &) {
+        iss_code = EXM_ERR_OOM;
+        iss_err = "store load: host memory exhausted";
+    } catch (const std::exception &e) {
+        iss_code = EXM_ERR_CUDA;
+        iss_err = std::string("store load: ") + e.what();
     }
     {
         std::lock_guard<std::mutex> lk(mu);

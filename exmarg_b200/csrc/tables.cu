@@ -237,6 +237,12 @@ extern "C" int exm_k_edges(exm_ctx *ctx, int n_max, int n_tau, const double *Wd,
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return 0;
 }
@@ -317,6 +323,12 @@ extern "C" int exm_bd_build(exm_ctx *ctx, int nord, int ntau, int nq, int nphif,
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return 0;
 }

@@ -288,6 +288,12 @@ extern "C" int exm_w_build(exm_ctx *ctx, int n_nodes, const double *s_nodes, int
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::bad_alloc &) {
+        ctx->err = "host memory exhausted";
+        return EXM_ERR_OOM;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return 0;
 }
