@@ -1,6 +1,6 @@
 """Stage 1 of the table build on the device (exm_w_build): the reference's own GORFs (golden w1), the
-oracle at n_max 20 (several tiles per phase class, partial tiles on both axes) and at 53 nodes (the
-production node count), build_w's files, and the refusal of a delay bin outside the grid.
+oracle at n_max 20 (several tiles per phase class, partial tiles on both axes), at 53 nodes (the
+production node count) and at 64 (every row of a tile), build_w's files, and the refusal of a delay bin outside the grid.
 
 Bars, relative to the largest |W| of each (node, key) over tau, beyond two float32 subnormal steps
 (at s = 0.01 the high orders are near 1e-40, where float32 keeps only a few bits, as the reference's
@@ -49,7 +49,8 @@ def test_reference_w():
 
 @pytest.mark.parametrize("s, n_max, nside, n_tau", [
     (np.geomspace(0.01, 200.0, 4), 20, 2, 33),
-    (np.geomspace(4.3e-3, 4000.0, 53), 3, 1, 9),
+    (np.geomspace(4.3e-3, 4000.0, 53), 3, 1, 9),      # the production node count
+    (np.geomspace(4.3e-3, 4000.0, 64), 3, 1, 9),      # every row of the 64-row tile
 ])
 def test_against_oracle(s, n_max, nside, n_tau):
     tau, W, _ = wtable.w_table(s, n_max, nside, n_tau)
