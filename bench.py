@@ -577,6 +577,58 @@ def w_build_leg(args, local):
     return out
 
 
+def shard_leg(args, store, seg, bank, local):
+    """node sharding projected on one GPU: the store's nodes split into 2, 4 and 8 ranges (node_ranges);
+    each range's node values for one segment (filter, time selection, taps, gather, lag log-sum-exp) timed
+    on a context of its own that holds only that range's tables, one range after another.  The slowest
+    range is the per-segment time of an N-GPU node-sharded run before its exchange (one all-reduce of
+    54 x 2048 float64 = 0.9 MB) and the node log-sum-exp on the host (timed here).  Timing only: a range's
+    tables are generated with range-local seeds (the device generator hashes a node's index in its store),
+    so their values differ from the whole store's; the work -- nodes, (node, template) pairs, taps -- is
+    the same."""
+    import exmarg_b200 as eb
+    from exmarg_b200 import _lib, shard as sh, synth
+    M, P, Q, S, seed = store.generator
+    nn = len(store.s)
+    rd = eb.read_segments(seg)
+
+    def time_range(k0, k1):
+        sub = synth.MemoryStore(store.spec, store.s[k0:k1], seed, tables=[None] * (k1 - k0))
+        sub.generator = (M, P, Q, S[k0:k1], seed)
+        if (k0, k1) != (0, nn):
+            sub.shard_s_before = float(store.s[k0 - 1]) if k0 > 0 else 0.0
+        ctx = _lib.Context(local)
+        try:
+            b = bank.clone_for(ctx)
+            eb.prepare(b, sub, "volume", 0.1267)
+            ts, lam = [], None
+            for rep in range(3):
+                e = rep % rd["rows"].size
+                t0 = time.perf_counter()
+                ctx.filter(rd["d_H"][e:e + 1], rd["d_L"][e:e + 1], rd["sig2_H"], rd["sig2_L"], want=False)
+                ctx.select_times(int(rd["rows"][e]), N_LOUD, N_RANDOM, want=False)
+                lam = ctx.node_values(k1 - k0)
+                ts.append(time.perf_counter() - t0)
+            return min(ts[1:]) * 1e3, lam
+        finally:
+            ctx.close()
+
+    full_ms, lam = time_range(0, nn)
+    lnW = sh.node_weights(store, np.asarray(bank.u, float), 0.1267, "volume")
+    t0 = time.perf_counter()
+    sh.combine(lam[None], lnW, bank.M, bank.q, bank.chi)
+    combine_ms = (time.perf_counter() - t0) * 1e3
+    out = {"whole_store_node_values_ms": full_ms, "host_combine_ms": combine_ms,
+           "exchange_estimate_ms": 0.02, "exchange": "0.9 MB all-reduce over NVLink (770 GB/s measured peer copy "
+           "on this pool), not run: one GPU per call here", "ranges": {}}
+    for n in (2, 4, 8):
+        ranges = sh.node_ranges(store, np.asarray(bank.u, float), 0.1267, n)
+        per = [time_range(k0, k1)[0] for k0, k1 in ranges]
+        out["ranges"][str(n)] = {"node_ranges": ranges, "ms_per_range": per, "slowest_ms": max(per),
+                                 "projected_segment_ms": max(per) + combine_ms + 0.02}
+    return out
+
+
 def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     """segments served by exmarg_b200.serve.Server: child contexts sharing the resident tables, three
     banks -- all 2048 templates on 8 s segments, the first 1024 on 16 s segments (n_time 65536), all 2048
@@ -730,6 +782,8 @@ def run_b200(args):
         line["redshift"] = redshift_leg(args, store, seg, local)
     if rank == 0 and world == 1 and args.io_nodes > 0:
         line["store_io"] = store_io_leg(args, local)
+    if rank == 0 and world == 1 and args.shard_legs:
+        line["node_shards"] = shard_leg(args, store, seg, bank, local)
     if rank == 0 and world == 1 and args.table_build:
         line["table_build"] = table_build_leg(args, local)
     if rank == 0 and world == 1 and args.w_pixels > 0:
@@ -780,6 +834,7 @@ def main():
     ap.add_argument("--prec-templates", type=int, default=64,
                     help="templates of the float64 oracle sample of the 16-bit table legs (0: no such legs)")
     ap.add_argument("--prec-steps", type=int, default=5, help="timed segments of each 16-bit table leg")
+    ap.add_argument("--shard-legs", type=int, default=1, help="node-sharding projection leg (0: no)")
     ap.add_argument("--only", choices=("all", "tables"), default="all",
                     help="'tables': only the offline table-build legs (no analysis, no JSON contract line)")
     ap.add_argument("--w-nodes", type=int, default=53, help="nodes of the stage-1 table-build leg")

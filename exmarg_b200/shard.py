@@ -2,7 +2,7 @@
 
 pe_intrinsic's node values -- ln Lambda of every template at every store node (exmarg/search/pe.py:168-200)
 -- need only that node's table, so the nodes split into contiguous ranges, one per rank, balanced by the
-(node, template) pairs each range covers.  A rank keeps only its range's tables in HBM (a store of 53
+gather work each range covers (its (node, template) pairs and a cost per node).  A rank keeps only its range's tables in HBM (a store of 53
 production nodes is 39.6 GB; a shard of it is 39.6/N) and computes its rows on the device: its context's
 store is declared a shard (exm_store_set_shard, the s of the node below the range), so the boundary point
 of the range's first node is set as the whole store sets it.  Every (node, template) value then comes from
@@ -44,14 +44,20 @@ def node_geometry(s, alpha_lo, alpha_hi, u, ymin):
     return valid, y, bnode
 
 
-def node_ranges(store, u, ymin, n_shards):
-    """n_shards contiguous node ranges [k0, k1), none empty, with about equal (node, template) pairs each
-    (a template's boundary point counts at its boundary node)"""
+# the gather's cost of a node beside that of its (node, template) pairs, in pairs: staging a node's windows
+# for every lag costs about as much as 3500 pairs (fit on a B200 at 2048 walked times, 87 lags: 1.43 ms a node,
+# 0.40 us a pair)
+NODE_WEIGHT = 3500.0
+
+
+def node_ranges(store, u, ymin, n_shards, node_weight=NODE_WEIGHT):
+    """n_shards contiguous node ranges [k0, k1), none empty, with about equal gather work each: the
+    (node, template) pairs (a template's boundary point counts at its boundary node) plus node_weight a node"""
     nn = len(store.s)
     if not 1 <= int(n_shards) <= nn:
         raise ValueError("need 1 <= shards <= %d (the store's nodes)" % nn)
     valid, _, bnode = node_geometry(store.s, store.alpha_lo, store.alpha_hi, u, ymin)
-    work = valid.sum(axis=1) + np.bincount(bnode[bnode >= 0], minlength=nn)[:nn] + 1.0
+    work = valid.sum(axis=1) + np.bincount(bnode[bnode >= 0], minlength=nn)[:nn] + float(node_weight)
     cum = np.concatenate([[0.0], np.cumsum(work)])
     cuts = [0]
     for i in range(1, int(n_shards)):
