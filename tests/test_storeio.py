@@ -78,3 +78,34 @@ def test_table_cli_orders_nodes_by_s(tmp_path):
     stems = tables.node_stems(str(tmp_path), "sladder_", ".meta.npz")
     assert [os.path.basename(t) for t in stems] == ["sladder_n120_s00000.004", "sladder_n120_s00003.000",
                                                    "sladder_n120_s00012.500"]
+
+
+def test_fortran_ordered_table_goes_through_host_memory(tmp_path):
+    """a T.npy member stored in Fortran order has no C-order byte range to stream: that node is sent from
+    its host copy, the others from their files"""
+    spec = synth.TableSpec(**SPEC)
+    s = synth.S_NODES_PROD[NODES[:2]]
+    synth.write_store(str(tmp_path), spec, s, SEED)
+    T = synth.gen_table_node(spec, 1, s, SEED)
+    f = sorted(str(p) for p in tmp_path.glob("bd_*.npz"))[1]
+    with np.load(f) as z:
+        members = {k: z[k] for k in z.files}
+    members["T"] = np.asfortranarray(T)
+    np.savez(f, **members)
+    st = eb.load_redshift_store(str(tmp_path), mmap=True)
+    assert st.t_offsets[0] is not None and st.t_offsets[1] is None
+    assert np.array_equal(st.tables[1], T)
+    ctx = FakeContext()
+    upload_store(st, ctx)
+    assert ctx.load["paths"] == [st.files[0], None]
+    assert ctx.load["hosts"][0] is None and ctx.load["hosts"][1] is st.tables[1]
+
+
+def test_compressed_store_is_refused(tmp_path):
+    spec = synth.TableSpec(**SPEC)
+    s = synth.S_NODES_PROD[NODES[:1]]
+    T = synth.gen_table_node(spec, 0, s, SEED)
+    np.savez_compressed(str(tmp_path / "bd_n120_s00001.000.npz"), T=T, beta=spec.beta, delta=spec.delta,
+                        tau_idx=spec.tau_idx, alpha=synth.ALPHA, s_node=float(s[0]))
+    with pytest.raises(ValueError, match="compressed"):
+        eb.load_redshift_store(str(tmp_path))
