@@ -144,3 +144,19 @@ def test_ranks_exchange_rows_over_gloo(fx_parts, world):
         assert np.array_equal(ln_lambda, got[0][1]) and np.array_equal(ln_b, got[0][2])
         assert np.allclose(ln_lambda, fx.ln_lambda, rtol=0, atol=1e-9)
         assert np.allclose(ln_b, fx.ln_b, rtol=0, atol=1e-9)
+
+
+def test_node_ranges_balance_the_work():
+    """the ranges' work (pairs plus NODE_WEIGHT a node) differs by at most about one node's work"""
+    import numpy as np
+    from exmarg_b200 import synth
+    s = synth.S_NODES_PROD
+    store = type("S", (), {})()
+    store.s, store.alpha_lo, store.alpha_hi = s, np.full(s.size, synth.ALPHA[0]), np.full(s.size, synth.ALPHA[-1])
+    u = np.geomspace(1.5, 3.0, 300)
+    valid, _, bnode = shard.node_geometry(store.s, store.alpha_lo, store.alpha_hi, u, 0.1267)
+    work = valid.sum(axis=1) + np.bincount(bnode[bnode >= 0], minlength=s.size)[:s.size] + shard.NODE_WEIGHT
+    for n in (2, 3, 4, 8, 16):
+        r = shard.node_ranges(store, u, 0.1267, n)
+        w = [work[a:b].sum() for a, b in r]
+        assert max(w) - min(w) <= 2 * work.max(), (n, w)
