@@ -5,7 +5,6 @@ import datetime
 import os
 import socket
 
-import pytest
 import torch.multiprocessing as mp
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
