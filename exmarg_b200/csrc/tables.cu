@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(256) k_bd_lse(const float *__restrict__ col, c
             for (int n = 0; n <= nm; ++n) mx = fmax(mx, __dadd_rn(__dmul_rn((double)n, be), g[n * kBdTile + j]));
             double tot = 0.0;
             for (int n = 0; n <= nm; ++n) {
-                const double e = __dadd_rn(__dmul_rn((double)n, be), g[n * kBdTile + j]);
-                tot = __dadd_rn(tot, exp(__dsub_rn(e, mx)));
+                const double e = __dsub_rn(__dadd_rn(__dmul_rn((double)n, be), g[n * kBdTile + j]), mx);
+                if (!(e <= -746.0)) tot = __dadd_rn(tot, exp(e));   // below, exp is exactly 0 (a NaN still adds)
             }
             const float t = (float)__dadd_rn(mx, log(tot));
             T[(size_t)l * per + at] = t;
