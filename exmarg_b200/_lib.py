@@ -23,7 +23,7 @@ GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2")
 # every symbol include/exmarg_b200.h declares
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
-           "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_set_times",
+           "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
            "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
 
@@ -69,6 +69,7 @@ def load():
         "exm_filter": ([P, P, P, P, P, P], I),
         "exm_set_trajectories": ([P, P], I),
         "exm_select_times": ([P, ctypes.c_int64, I, I, P, P], I),
+        "exm_np_exp32": ([P, P, P, ctypes.c_int64], I),
         "exm_set_times": ([P, I, P, P], I),
         "exm_gather": ([P, I, I, P, P, P, P], I),
         "exm_node_values": ([P, P], I),
@@ -351,6 +352,13 @@ class Context:
         lw = np.empty((self.nm, nw), np.float32) if want else None
         self._check(self.lib.exm_select_times(self.h, int(seed), int(n_loud), int(n_random), _p(sel), _p(lw)))
         return (sel, lw) if want else None
+
+    def np_exp32(self, x):
+        """numpy's float32 exp evaluated on the device (the selection score's exp)"""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty_like(x)
+        self._check(self.lib.exm_np_exp32(self.h, _p(x), _p(y), x.size))
+        return y
 
     def set_times(self, times):
         if times is None:

@@ -18,6 +18,8 @@ void exm_run_node_values(exm_ctx *ctx, exm_slot &sl, double *d_lamN);
 void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,
                                 const double *d_p, int n_dens);
 void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
+void exm_run_np_exp32(exm_ctx *ctx, const float *d_x, float *d_y, long long n);
+void exm_noalloc_load(int dev);
 
 // ------------------------------------------------------------------ memory
 
@@ -229,6 +231,7 @@ extern "C" int exm_ctx_create(int device, size_t hbm_budget, exm_ctx **out)
         size_t fr = 0, tot = 0;
         EXM_CUDA(cudaMemGetInfo(&fr, &tot));
         ctx->budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+        exm_noalloc_load(device);   // exm_gather_noalloc's fixed scratch and kernels, loaded now
     } catch (const exm_error &e) {
         fprintf(stderr, "exm_ctx_create: %s\n", e.msg.c_str());
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1198,6 +1201,23 @@ extern "C" int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_ra
             }
         }
     }
+    API_END(ctx)
+}
+
+extern "C" int exm_np_exp32(exm_ctx *ctx, const float *x, float *y, int64_t n)
+{
+    API_BEGIN(ctx)
+    EXM_CUDA(cudaSetDevice(ctx->dev));
+    REQUIRE(n >= 0 && (n == 0 || (x && y)), EXM_ERR_ARG, "bad exp arguments");
+    if (n == 0) return EXM_OK;
+    dbuf dx;
+    exm_alloc(ctx, dx, sizeof(float) * 2 * (size_t)n);
+    float *d_x = (float *)dx.p, *d_y = d_x + n;
+    EXM_CUDA(cudaMemcpyAsync(d_x, x, sizeof(float) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+    exm_run_np_exp32(ctx, d_x, d_y, (long long)n);
+    EXM_CUDA(cudaMemcpyAsync(y, d_y, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    EXM_CUDA(cudaStreamSynchronize(ctx->stream));
+    exm_free(ctx, dx);
     API_END(ctx)
 }
 

@@ -8,12 +8,18 @@
 //
 // The array is part of the library image: every device that loads the library holds it
 // (16 MiB + 256 B) until the process exits.  Host code must not hand the array's name
-// to a kernel (it is a host-side stand-in, not a device address); the device address is
-// looked up once per device with cudaGetSymbolAddress, on the first call made on that
-// device, and reused afterwards -- make that first call before any stream capture.  All
-// calls share the array and it keeps the previous call's contents; the error word is
-// cleared at the start of every call, and two calls that overlap on the GPU (two
-// contexts or streams at once) race on it.
+// to a kernel (it is a host-side stand-in, not a device address).  With CUDA's lazy
+// module loading the array and the kernels of this file would only be loaded -- device
+// memory allocated -- on their first use, so exm_ctx_create loads them (exm_noalloc_load):
+// it looks the device addresses up with cudaGetSymbolAddress, with the context's device
+// current, and queries every kernel of this file.  The addresses are looked up again by
+// every context creation on the device (a device reset between contexts gets fresh
+// ones); they assume the device's primary context outlives the contexts created on it.
+// A call made without a context creation on its device since the process started (not
+// possible through this ABI) would look them up itself; make the first call before any
+// stream capture.  All calls share the array and it keeps the previous call's contents;
+// the error word is cleared at the start of every call, and two calls that overlap on
+// the GPU (two contexts or streams at once) race on it.
 #include <mutex>
 
 #include "common.cuh"
@@ -31,12 +37,13 @@ static std::mutex g_noalloc_mu;
 static double *g_noalloc_addr[EXM_NOALLOC_MAX_DEVICES];
 static unsigned *g_noalloc_err_addr[EXM_NOALLOC_MAX_DEVICES];
 
-// the device addresses of the scratch array and the error word on device dev (current)
-static void noalloc_addresses(int dev, double **scratch, unsigned **err)
+// the device addresses of the scratch array and the error word on device dev (current);
+// refresh: look them up again even if known
+static void noalloc_addresses(int dev, double **scratch, unsigned **err, bool refresh = false)
 {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     if (dev < 0 || dev >= EXM_NOALLOC_MAX_DEVICES) EXM_THROW(EXM_ERR_ARG, "device index out of range");
-    if (!g_noalloc_addr[dev]) {
+    if (refresh || !g_noalloc_addr[dev]) {
         void *p = nullptr, *q = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
@@ -155,6 +162,20 @@ __global__ void k_gather_noalloc_lags(const double *__restrict__ om, const doubl
     out[idx] = mx + log(tot) - log((double)nt);
 }
 
+// Called by exm_ctx_create with device dev current: loads this file's module (the scratch array) and its
+// kernels now, so that exm_gather_noalloc allocates nothing on its first call either.
+void exm_noalloc_load(int dev)
+{
+    double *scratch = nullptr;
+    unsigned *err = nullptr;
+    noalloc_addresses(dev, &scratch, &err, true);
+    cudaFuncAttributes fa;
+    EXM_CUDA(cudaFuncGetAttributes(&fa, (const void *)k_gather_noalloc<float>));
+    EXM_CUDA(cudaFuncGetAttributes(&fa, (const void *)k_gather_noalloc<__half>));
+    EXM_CUDA(cudaFuncGetAttributes(&fa, (const void *)k_gather_noalloc<__nv_bfloat16>));
+    EXM_CUDA(cudaFuncGetAttributes(&fa, (const void *)k_gather_noalloc_lags));
+}
+
 extern "C" int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float *lqH, const float *phH,
                                   const float *lqL, const float *phL, int nwalk, const int32_t *sel, const float *lw,
                                   int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,
@@ -230,6 +251,9 @@ extern "C" int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float 
     } catch (const exm_error &e) {
         ctx->err = e.msg;
         return e.code;
+    } catch (const std::exception &e) {
+        ctx->err = e.what();
+        return EXM_ERR_CUDA;
     }
     return EXM_OK;
 }

@@ -4,10 +4,12 @@
 //   (in time order) with numpy's default_rng(seed).integers(0, n_time - n_loud,
 //   (n_template, n_random)), each with log weight ln((n_time - n_loud) / n_random);
 //   the visited times are returned sorted.
-// Ties at the n_loud-th score are broken by time (earliest first); numpy's
+// The score's exp is numpy's float32 exp restated bit for bit (npexp.cuh), so equal trajectories give
+// equal scores.  Ties at the n_loud-th score are broken by time (earliest first); numpy's
 // argpartition leaves that order unspecified.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "npexp.cuh"
 #include "pcg64.cuh"
 
 #define SCORE_TILE 2048
@@ -44,7 +46,7 @@ __global__ void __launch_bounds__(256) k_scores(const float2 *__restrict__ trajH
         const int t = t0 + j;
         if (t >= nt) break;
         const float mx = fmaxf(a[j], a[j + wn - w]);
-        const float s = __fadd_rn(expf(2.0f * Lr[t].x), expf(2.0f * mx));
+        const float s = __fadd_rn(exm_np_expf(2.0f * Lr[t].x), exm_np_expf(2.0f * mx));
         keys[(long long)m * nt + t] = __float_as_uint(s);
     }
 }
@@ -344,4 +346,20 @@ void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk,
                                                d_order_chunk, nt, K, S, Sp, (int32_t *)sl.sel.p);
     EXM_CUDA(cudaGetLastError());
     ctx->launches += 2;
+}
+
+// ------------------------------------------------------------------ the score's exp, for tests
+
+__global__ void k_np_exp32(const float *__restrict__ x, float *__restrict__ y, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = exm_np_expf(x[i]);
+}
+
+void exm_run_np_exp32(exm_ctx *ctx, const float *d_x, float *d_y, long long n)
+{
+    if (n <= 0) return;
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 16);
+    k_np_exp32<<<(unsigned)blocks, 256, 0, ctx->stream>>>(d_x, d_y, n);
+    EXM_CUDA(cudaGetLastError());
 }

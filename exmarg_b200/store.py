@@ -17,6 +17,7 @@ import struct
 import zipfile
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
+from typing import NamedTuple
 
 import numpy as np
 
@@ -25,33 +26,53 @@ from . import _lib
 NPHI = 96
 
 
-def _member_offset(path, name):
-    info = zipfile.ZipFile(path).getinfo(name)
-    if info.compress_type != 0:
+class MemberLayout(NamedTuple):
+    """where an array member's raw bytes lie inside an .npz and how to read them"""
+    offset: int            # byte offset of the array data in the archive file
+    shape: tuple
+    fortran: bool
+    dtype: np.dtype
+
+
+_LOCAL_HEADER = struct.Struct("<4s22xHH")    # zip local file header: signature, ..., name length, extra length
+_NPY_HEADERS = {(1, 0): np.lib.format.read_array_header_1_0, (2, 0): np.lib.format.read_array_header_2_0}
+
+
+def npz_member_layout(path, name):
+    """The layout of the uncompressed member `name` (an .npy file) of the zip archive `path`.
+
+    The archive's central directory gives the member's local header position; the data follow the
+    30-byte local header and its variable name and extra fields (their lengths are the header's last
+    two little-endian 16-bit fields).  The data start with the .npy preamble (magic, version, the
+    header dictionary with shape, order and dtype); the array bytes come right after it, so they can
+    be read with one sequential read, mapped, or handed to a native loader by offset.  A compressed
+    member has no such byte range and is refused (ValueError), as the reference's reader refuses it."""
+    with zipfile.ZipFile(path) as zf:
+        info = zf.getinfo(name)
+    if info.compress_type != zipfile.ZIP_STORED:
         raise ValueError("member %s of %s is compressed" % (name, path))
     with open(path, "rb") as fh:
         fh.seek(info.header_offset)
-        nlen, elen = struct.unpack("<HH", fh.read(30)[26:30])
-        fh.seek(info.header_offset + 30 + nlen + elen)
-        ver = np.lib.format.read_magic(fh)
-        rd = np.lib.format.read_array_header_1_0 if ver == (1, 0) else np.lib.format.read_array_header_2_0
-        shape, fortran, dtype = rd(fh)
-        return fh.tell(), shape, fortran, dtype
+        sig, n_name, n_extra = _LOCAL_HEADER.unpack(fh.read(_LOCAL_HEADER.size))
+        if sig != b"PK\x03\x04":
+            raise ValueError("no zip local header for %s in %s" % (name, path))
+        fh.seek(info.header_offset + _LOCAL_HEADER.size + n_name + n_extra)
+        version = np.lib.format.read_magic(fh)
+        if version not in _NPY_HEADERS:
+            raise ValueError("unsupported .npy version %s in %s" % (version, path))
+        shape, fortran, dtype = _NPY_HEADERS[version](fh)
+        return MemberLayout(fh.tell(), tuple(shape), bool(fortran), np.dtype(dtype))
 
 
-def read_npz_member(path, name):
-    """one uncompressed .npy member of an npz, read sequentially"""
-    off, shape, fortran, dtype = _member_offset(path, name)
-    with open(path, "rb") as fh:
-        fh.seek(off)
-        arr = np.fromfile(fh, dtype=dtype, count=int(np.prod(shape)))
-    return arr.reshape(shape, order="F" if fortran else "C")
-
-
-def map_npz_member(path, name):
-    """read-only memory map of one uncompressed .npy member of an npz"""
-    off, shape, fortran, dtype = _member_offset(path, name)
-    return np.asarray(np.memmap(path, dtype=dtype, mode="r", offset=off, shape=shape, order="F" if fortran else "C"))
+def npz_member(path, name, mmap=False):
+    """the array of member `name` of the .npz `path`: read into memory, or a read-only map (mmap=True)"""
+    lay = npz_member_layout(path, name)
+    order = "F" if lay.fortran else "C"
+    if mmap:
+        return np.asarray(np.memmap(path, dtype=lay.dtype, mode="r", offset=lay.offset, shape=lay.shape, order=order))
+    count = int(np.prod(lay.shape))
+    arr = np.fromfile(path, dtype=lay.dtype, count=count, offset=lay.offset)
+    return arr.reshape(lay.shape, order=order)
 
 
 @dataclass
@@ -80,8 +101,8 @@ TABLE_DTYPES = {"f32": _lib.DTYPE_F32, "f16": _lib.DTYPE_F16, "bf16": _lib.DTYPE
 
 def _table_offset(path):
     """byte offset of the T.npy data in a bd_*.npz when it is float32 in C order (else None)"""
-    off, shape, fortran, dtype = _member_offset(path, "T.npy")
-    return off if (np.dtype(dtype) == np.dtype("<f4") and (not fortran or len(shape) <= 1)) else None
+    lay = npz_member_layout(path, "T.npy")
+    return lay.offset if (lay.dtype == np.dtype("<f4") and (not lay.fortran or len(lay.shape) <= 1)) else None
 
 
 def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dtype="f32", direct=False):
@@ -104,10 +125,10 @@ def load_redshift_store(store_dir, pinned=False, readers=6, mmap=False, table_dt
     head.sort(key=lambda r: r[0])
     s, alo, ahi, beta, delta, tau, files = zip(*head)
     if mmap:
-        tables = [map_npz_member(f, "T.npy") for f in files]
+        tables = [npz_member(f, "T.npy", mmap=True) for f in files]
     else:
         with ThreadPoolExecutor(max_workers=max(1, int(readers))) as ex:
-            tables = list(ex.map(lambda f: read_npz_member(f, "T.npy"), files))
+            tables = list(ex.map(lambda f: npz_member(f, "T.npy"), files))
     return RedshiftStore(s=np.array(s), alpha_lo=np.array(alo), alpha_hi=np.array(ahi), beta=list(beta),
                          delta=list(delta), tau_idx=tau[0], tables=tables,
                          n_max=int(os.path.basename(files[0]).split("_n")[1].split("_")[0]), table_dtype=table_dtype,

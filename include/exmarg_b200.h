@@ -260,6 +260,11 @@ EXM_API int exm_set_trajectories(exm_ctx *ctx, const float *traj);
  * float32, if not NULL, receive the result. */
 EXM_API int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_random, int32_t *sel_out, float *lw_out);
 
+/* The float32 exp the selection scores use, on the device: y[i] = exp(x[i]) for n host values,
+ * bit for bit numpy's float32 np.exp (its SIMD kernel on AVX2 / AVX-512 hosts), the exp of the
+ * reference's score (exmarg/search/gather.py:407).  For tests of the selection's arithmetic. */
+EXM_API int exm_np_exp32(exm_ctx *ctx, const float *x, float *y, int64_t n);
+
 /* Upload a time selection (nm, nwalk) from the host in place of exm_select_times
  * (nwalk = 0: every arrival time). */
 EXM_API int exm_set_times(exm_ctx *ctx, int nwalk, const int32_t *sel, const float *lw);
@@ -281,11 +286,14 @@ EXM_API int exm_gather(exm_ctx *ctx, int nsel, int ns, const int64_t *mass_ids, 
  * (nsel, ns) int64 node indices into the context's resident store; out (ns, nsel)
  * float64.  The call allocates nothing: its partial sums live in a fixed device array
  * of the library (16 MiB, held by every device that loads the library), so
- * ns * n_lag * nsel must not exceed 2^20 (larger requests fail with EXM_ERR_ARG).  The
- * first call on a device looks the array's device address up (cudaGetSymbolAddress);
- * make it before any stream capture.  Calls share the array: two calls that overlap on
- * the GPU race.  It runs on the context's stream and returns after the result is
- * written. */
+ * ns * n_lag * nsel must not exceed 2^20 (larger requests fail with EXM_ERR_ARG).
+ * exm_ctx_create loads the array and this call's kernels on its device and looks the
+ * array's device address up (cudaGetSymbolAddress), so no call allocates, the first
+ * included; the address is refreshed by every context creation and assumes the device's
+ * primary context outlives the contexts.  Calls share the array and its error word: do
+ * not run two calls at once on one device (two contexts or streams); they would race.
+ * Out-of-range mass ids, table ids or visited times fail with EXM_ERR_ARG.  It runs on
+ * the context's stream and returns after the result is written. */
 EXM_API int exm_gather_noalloc(exm_ctx *ctx, int nm, int n_time, const float *lqH, const float *phH,
                                const float *lqL, const float *phL, int nwalk, const int32_t *sel, const float *lw,
                                int nsel, int ns, const int64_t *mass_ids, const double *lna, const int64_t *tab_ids,

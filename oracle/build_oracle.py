@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_build", "liboracle.so")
 
 
-SOURCES = ("gather_fp64.c", "gen_tables.c")
+SOURCES = ("gather_fp64.c", "gen_tables.c", "npexp.c")
 
 
 def build(force=False):

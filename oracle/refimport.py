@@ -8,6 +8,9 @@ empty stand-in modules are registered for them first; the only lalsuite use on
 the analysed path is the template profile (exmarg/profiles.py:26-47), which is
 replaced by exmarg_b200.synth.profile (same return signature).  numba caches are
 sent to a writable directory because the reference tree is read-only.
+
+The source tree (the directory holding the `exmarg` package) is named by the
+EXMARG_REFERENCE_SRC environment variable or passed as an argument.
 """
 
 import os
@@ -15,17 +18,24 @@ import sys
 import tempfile
 import types
 
-DEFAULT_SRC = "/root/reference/src"
+ENV = "EXMARG_REFERENCE_SRC"
 
 
-def available(src=DEFAULT_SRC):
-    return os.path.isdir(os.path.join(src, "exmarg", "search"))
+def source_dir(src=None):
+    """the reference source directory: the argument, else $EXMARG_REFERENCE_SRC (None if neither)"""
+    return src or os.environ.get(ENV) or None
 
 
-def import_reference(src=DEFAULT_SRC):
+def available(src=None):
+    src = source_dir(src)
+    return bool(src) and os.path.isdir(os.path.join(src, "exmarg", "search"))
+
+
+def import_reference(src=None):
     """the reference's exmarg.search module, with the TaylorF2 profile patched in"""
+    src = source_dir(src)
     if not available(src):
-        raise ImportError("reference source tree not found at %s" % src)
+        raise ImportError("reference source tree not found (pass its src directory or set %s); got %r" % (ENV, src))
     os.environ.setdefault("NUMBA_CACHE_DIR", os.path.join(tempfile.gettempdir(), "exmarg_ref_numba"))
     for name in ("healpy", "lal", "lalsimulation"):
         if name not in sys.modules:

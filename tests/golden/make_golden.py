@@ -2,7 +2,7 @@
 code (exmarg.search: numpy + numba; its table builders scripts/build_tables/w_gpu.py, build_k.py and
 build_bd.py, w_gpu.py with numpy standing in for cupy) in a container where its source tree is present.
 
-    python tests/golden/make_golden.py [reference src dir [case ...]]
+    python tests/golden/make_golden.py <reference src dir, or - for $EXMARG_REFERENCE_SRC> [case ...]
 
 Each fixture holds the inputs (segments, bank rows, W and u, the store geometry and the
 float32 generator factors of its seeded tables) and the reference's outputs (ln_lambda,
@@ -24,7 +24,7 @@ from exmarg_b200 import synth  # noqa: E402
 from oracle import refimport  # noqa: E402
 
 CASES = {
-    # BASELINE config 1 shape: 8 s, analysis band 20-256 Hz (lag unit 1/2048 s, lags +-21),
+    # the reduced CPU case: 8 s, analysis band 20-256 Hz (lag unit 1/2048 s, lags +-21),
     # 3 nodes at reduced beta/Delta settings, 64 templates
     "config1": dict(T=8.0, fmax=256.0, ntau=43, nb=100, nd=109, nodes=(14, 24, 34), n_template=64, n_seg=2,
                     snr=15.0, n_loud=1024, n_random=1024, seed_seg=100, seed_bank=3, seed_tab=7, prior="volume"),
@@ -267,7 +267,10 @@ def make_k(name, c, ref_root):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else refimport.DEFAULT_SRC
+    # the reference's src directory: first argument, else $EXMARG_REFERENCE_SRC
+    src = refimport.source_dir(sys.argv[1] if len(sys.argv) > 1 and sys.argv[1] != "-" else None)
+    if src is None:
+        sys.exit("usage: make_golden.py <reference src dir | -> [case ...]  (or set %s)" % refimport.ENV)
     only = sys.argv[2:] if len(sys.argv) > 2 else None
     if only is None or any(n in only for n in list(CASES) + list(REDSHIFT_CASES)):
         search = refimport.import_reference(src)
