@@ -21,7 +21,7 @@ PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2")
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
@@ -56,6 +56,7 @@ def load():
         "exm_ctx_create_sharing": ([P, Z, ctypes.POINTER(P)], I),
         "exm_ctx_set_graph": ([P, I], I),
         "exm_ctx_set_priority": ([P, I, P], I),
+        "exm_ctx_test_wait_expiry": ([P, I], I),
         "exm_last_error": ([P], ctypes.c_char_p),
         "exm_ctx_bytes": ([P], Z),
         "exm_ctx_timing": ([P, I, P], I),
@@ -148,6 +149,10 @@ class Context:
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
         self._check(self.lib.exm_ctx_set_graph(self.h, 1 if enable else 0))
+
+    def test_wait_expiry(self, enable=True):
+        """test support: the plane gather stages nothing, so its bounded waits run out (EXM_ERR_TIMEOUT)"""
+        self._check(self.lib.exm_ctx_test_wait_expiry(self.h, 1 if enable else 0))
 
     def set_priority(self, priority):
         """stream priority (0 default, lower numbers first; clamped); returns the device's

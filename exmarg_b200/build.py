@@ -4,6 +4,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libexmarg_b200.so")
@@ -34,15 +35,19 @@ def build(force=False, verbose=False):
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         cmd = [NVCC] + FLAGS + ["-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.check_call, cmd) for cmd, _ in jobs]:
+            f.result()
+    objs = [obj for _, obj in jobs]
     link = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + objs + [
         "-cudart", "static", "-L" + os.path.join(CUDA, "lib64"), "-lcufft",
         "-Xlinker", "-rpath," + os.path.join(CUDA, "lib64")]

@@ -8,6 +8,8 @@
 
 #include <mutex>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "pcg64.cuh"
@@ -881,22 +883,38 @@ static void check_dev_err(exm_ctx *ctx, exm_slot &sl)
     if (e & EXM_DEVERR_BOUNDS) EXM_THROW(EXM_ERR_CUDA, "a tap descriptor pointed outside its block (internal error)");
 }
 
+// NVTX range of one pipeline stage on the calling host thread (the launches it encloses show up under it in
+// a timeline profiler); free when no profiler is attached
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 // everything of one segment from the staged input to lnl / lnb on the device
 static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
 {
+    NvtxRange seg_range("exm segment");
     const int tt = exm_tim_begin(ctx, 0);
     EXM_CUDA(cudaMemsetAsync(sl.dev_err.p, 0, sizeof(unsigned), ctx->stream));
     if (rs.K > 0) {
+        NvtxRange nr("exm select: random draws");
         const int h = exm_tim_begin(ctx, 2);
         exm_run_pcg(ctx, sl, state_words(ctx, sl), rs.K, rs.S);
         exm_tim_end(ctx, h);
     }
     for (int m_base = 0; m_base < ctx->nm; m_base += rs.nmc_max) {
         const int nmc = std::min(rs.nmc_max, ctx->nm - m_base);
-        int h = exm_tim_begin(ctx, 1);
-        exm_run_filter(ctx, sl, (const float2 *)ctx->d_W.p + (size_t)m_base * ctx->nfreq, nmc);
-        exm_tim_end(ctx, h);
+        int h;
+        {
+            NvtxRange nr("exm filter");
+            h = exm_tim_begin(ctx, 1);
+            exm_run_filter(ctx, sl, (const float2 *)ctx->d_W.p + (size_t)m_base * ctx->nfreq, nmc);
+            exm_tim_end(ctx, h);
+        }
         if (rs.K > 0) {
+            NvtxRange nr("exm select");
             h = exm_tim_begin(ctx, 2);
             exm_run_topk(ctx, sl, nmc, (const int *)ctx->d_order.p + m_base, rs.K, rs.S);
             exm_tim_end(ctx, h);
@@ -904,17 +922,23 @@ static void run_segment(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
         ChunkInfo ci{m_base, nmc, rs.nwalk, rs.use_sel, rs.lw};
         for (int r0 = 0; r0 < ctx->ntau; r0 += rs.rc) {
             const int rc = std::min(rs.rc, ctx->ntau - r0);
-            h = exm_tim_begin(ctx, 3);
-            exm_run_taps(ctx, sl, ci, r0, rc, r0 == 0);
-            exm_tim_end(ctx, h);
+            {
+                NvtxRange nr("exm taps");
+                h = exm_tim_begin(ctx, 3);
+                exm_run_taps(ctx, sl, ci, r0, rc, r0 == 0);
+                exm_tim_end(ctx, h);
+            }
+            NvtxRange nr("exm gather");
             h = exm_tim_begin(ctx, 4);
             exm_run_gather_planes(ctx, sl, ci, r0, rc);
             exm_tim_end(ctx, h);
         }
+        NvtxRange nr("exm epilogue");
         h = exm_tim_begin(ctx, 5);
         exm_run_node_lse(ctx, sl, m_base, nmc);
         exm_tim_end(ctx, h);
     }
+    NvtxRange nr("exm epilogue: ln B");
     const int h = exm_tim_begin(ctx, 5);
     exm_run_lnb(ctx, sl);
     exm_tim_end(ctx, h);
@@ -973,6 +997,7 @@ static void run_segment_graph(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
         memcpy(ctx->graph_key, key, sizeof(key));
         return;
     }
+    NvtxRange nr("exm segment (graph replay)");
     const int h = exm_tim_begin(ctx, 0);
     EXM_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
     exm_tim_end(ctx, h);
@@ -1201,6 +1226,14 @@ extern "C" int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_ra
             }
         }
     }
+    API_END(ctx)
+}
+
+extern "C" int exm_ctx_test_wait_expiry(exm_ctx *ctx, int enable)
+{
+    API_BEGIN(ctx)
+    ctx->test_wait_expiry = enable != 0;
+    ctx->graph_key[0] = -1;   // a captured graph holds the old launch arguments
     API_END(ctx)
 }
 

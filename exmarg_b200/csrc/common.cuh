@@ -129,7 +129,8 @@ struct exm_ctx {
     // launch shape of the plane gather (index into its table; chosen by exm_autotune)
     struct exm_redshift *rs = nullptr;   // pe_redshift's grid and buffers (csrc/redshift.cu)
     int gather_cfg = 0;
-    int gather_chunk_pct = 100;   // templates per gather block, percent of the one-wave-per-lag size
+    int gather_chunk_pct = 100;
+    bool test_wait_expiry = false;   // the plane gather stages nothing and its barrier waits run out (a test)   // templates per gather block, percent of the one-wave-per-lag size
 
     // cuFFT
     cufftHandle plan = 0;

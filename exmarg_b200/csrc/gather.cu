@@ -31,6 +31,7 @@ template <typename TE> __host__ __device__ constexpr int slot_elems() { return E
 template <typename TE> __host__ __device__ constexpr unsigned slot_bytes() { return (unsigned)(slot_elems<TE>() * sizeof(TE)); }
 static_assert(slot_bytes<float>() % 128 == 0 && slot_bytes<__half>() % 128 == 0, "slots keep 128-byte alignment");
 #define EXM_WAIT_CYCLES (2000000000LL)   // about one second at 1.9 GHz
+#define EXM_TEST_WAIT_CYCLES (20000LL)   // the wait-expiry test's limit (no copy is ever in flight then)
 
 struct PlaneArgs {
     const uint4 *desc;
@@ -47,6 +48,9 @@ struct PlaneArgs {
     int nn, ntau, nphif, nb, nd, ndp, nt, nmc, m_base, nm_total, r0, tch, nch;
     float lw;
     double rph, rdb, rdd, offd;
+    long long wait_cycles;       // limit of the pipeline's barrier waits (EXM_WAIT_CYCLES)
+    int stage;                   // 1: stage the planes; 0 (the wait-expiry test): no copy is issued, so the
+                                 // first wait runs out and the kernel returns its timeout status
     int cki[EXM_MAX_NODES];
     float ckf[EXM_MAX_NODES];
     float tsc[EXM_MAX_NODES];    // per node: value = tsc * stored element
@@ -75,8 +79,9 @@ __device__ __forceinline__ void tma_load_plane(const CUtensorMap *map, uint64_t 
 }
 
 
-// bounded wait on a phase of an mbarrier; false (and the error word set) if it ran out
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err)
+// bounded wait on a phase of an mbarrier; false (and the error word set) if it ran out after `limit` cycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned *err,
+                                          long long limit = EXM_WAIT_CYCLES)
 {
     const uint32_t a = smem_u32(bar);
     const long long t0 = clock64();
@@ -88,7 +93,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsign
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > EXM_WAIT_CYCLES) {
+        if (clock64() - t0 > limit) {
             atomicOr(err, EXM_DEVERR_TIMEOUT);
             return false;
         }
@@ -547,20 +552,22 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         // ---------------------------------------------------------------- producer
         const int32_t *tsr_all = a.tside + (long long)rl * a.per_lag;
         int issued = 0;
-        if (lane == 0)
-            for (int q = 0; q < 3 && q < a.nphif; ++q)
-                tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
-        issued = min(3, a.nphif);
+        if (a.stage) {
+            if (lane == 0)
+                for (int q = 0; q < 3 && q < a.nphif; ++q)
+                    tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
+            issued = min(3, a.nphif);
+        }
         bool ok = true;
         for (int p = 0; p < EXM_NPAIR; ++p) {
-            ok = ok && __all_sync(0xffffffffu, mbar_wait(&done[p & 1], (p >> 1) & 1, a.err));
+            ok = ok && __all_sync(0xffffffffu, mbar_wait(&done[p & 1], (p >> 1) & 1, a.err, a.wait_cycles));
             if (!ok) break;
             fold_edges(gsm_f(edge_off(p & 1, 0)), NC, acc + 6 * tch, acc + 7 * tch, acc + 8 * tch, n);
             if (blo < bhi)
                 fold_edges(gsm_f(edge_off(p & 1, 1)), NC, acc + 15 * tch, acc + 16 * tch, acc + 17 * tch, n);
             __syncwarp();
             // plane p is no longer needed anywhere: its slot takes plane p + 3
-            if (p + 3 < a.nphif) {
+            if (a.stage && p + 3 < a.nphif) {
                 if (lane == 0) tma_load_plane(&tmap, &full[p % 3], win + (p % 3) * SLOT, C0, R0, p + 3, r, k, SLOT_B);
                 ++issued;
             }
@@ -620,7 +627,8 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         if (!ok) {
             if (lane == 0) {
                 atomicOr(&bad_sh, 1u);
-                // drain: the newest copy of each slot completes after the older ones of that slot (bounded)
+                // drain: the newest copy of each slot completes after the older ones of that slot (bounded by
+                // the full limit whatever the pipeline's: the block must not exit with a copy in flight)
                 for (int q = max(0, issued - 3); q < issued; ++q) mbar_wait(&full[q % 3], (q / 3) & 1, a.err);
             }
         }
@@ -649,8 +657,9 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         bool ok = true;
         for (int p = 0; p < EXM_NPAIR; ++p) {
             // warp-uniform: the lanes go on to shuffles together
-            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err));
-            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err));
+            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err, a.wait_cycles));
+            ok = ok && __all_sync(0xffffffffu,
+                                  mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err, a.wait_cycles));
             if (lane == 0) qcnt[(p % 3) * 32 + warp] = 0;
             __syncwarp();
             rc.qn = qcnt_o + 4u * ((p % 3) * 32 + warp);
@@ -801,6 +810,8 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.rdb = 2.0 / ctx->dbeta;
     a.rdd = 1.0 / ctx->ddelta;
     a.offd = -ctx->delta0 / ctx->ddelta;
+    a.stage = ctx->test_wait_expiry ? 0 : 1;
+    a.wait_cycles = ctx->test_wait_expiry ? EXM_TEST_WAIT_CYCLES : EXM_WAIT_CYCLES;
     for (int k = 0; k < ctx->nn; ++k) {
         const double f = std::floor(ctx->ck[k]);
         a.cki[k] = (int)f;

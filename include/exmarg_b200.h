@@ -77,6 +77,13 @@ EXM_API int exm_ctx_set_graph(exm_ctx *ctx, int enable);
  * (which multiplies the tap descriptors resident in L2).  No reference counterpart. */
 EXM_API int exm_ctx_set_priority(exm_ctx *ctx, int priority, int *range_out);
 EXM_API const char *exm_last_error(const exm_ctx *ctx);
+
+/* Test support for failure detection (no reference counterpart).  enable = 1: the plane gather of
+ * this context issues no table copy, so its first bounded barrier wait runs out (after ~20k cycles
+ * instead of ~1 s); the kernel then sets the device error word and returns, and the call fails with
+ * EXM_ERR_TIMEOUT while the context stays usable.  No copy is in flight when a block exits.
+ * enable = 0 restores normal operation. */
+EXM_API int exm_ctx_test_wait_expiry(exm_ctx *ctx, int enable);
 /* Bytes of device memory the context holds now. */
 EXM_API size_t exm_ctx_bytes(const exm_ctx *ctx);
 
