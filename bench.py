@@ -152,16 +152,73 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per plane-gather launch of the full workload, from the committed ncu launch list"""
-    path = os.path.join(ROOT, "profiles", "launches_pe_intrinsic_prod.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+# DRAM traffic of the plane gather, per node-tap, from one ncu capture of a reduced case (one kernel, one
+# launch, a few GB on the device: profiles/k_gather_planes_small.md gives the command).  The bytes a launch
+# moves scale with its node-taps (the windows staged per (node, lag, template block) and the descriptors
+# read per node-tap both do), so the full launch's traffic is this figure times its node-taps.  The capture
+# holds only for the kernel sources it was taken on: if they changed since, traffic is reported as null.
+GATHER_TRAFFIC = {
+    "dram_bytes_per_node_tap": None,
+    "l2_read_hit_rate": None,
+    "sources_sha256": None,
+    "capture": "profiles/k_gather_planes_small.md",
+}
+GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh",
+                  "exmarg_b200/csrc/common.cuh")
+
+
+def gather_sources_sha256():
+    import hashlib
+    h = hashlib.sha256()
+    for f in GATHER_SOURCES:
+        with open(os.path.join(ROOT, f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()
+
+
+def gather_traffic(node_taps_per_launch):
+    """(DRAM bytes per launch scaled from the reduced-case capture, L2 read hit rate, why null)"""
+    g = GATHER_TRAFFIC
+    if g["dram_bytes_per_node_tap"] is None:
+        return None, None, "no capture recorded"
+    if g["sources_sha256"] != gather_sources_sha256():
+        return None, None, "stale: the gather sources changed since the capture"
+    return g["dram_bytes_per_node_tap"] * node_taps_per_launch, g["l2_read_hit_rate"], None
+
+
+def compulsory_table_bytes(traj, sel, u, spec, s_nodes, lags):
+    """A lower bound on the table bytes one segment's gather must read from DRAM: the distinct 32-byte
+    sectors of the node tables that the taps of a template sample touch (every tap reads 2 phase planes x
+    2 beta rows x 2 Delta columns at every node it reaches), counted on the host for the sampled lags and
+    scaled to all lags.  A sample touches no more sectors than the whole bank, so this bounds the full
+    workload's compulsory table bytes from below."""
+    nphi = 96
+    db, dd = spec.beta[1] - spec.beta[0], spec.delta[1] - spec.delta[0]
+    nt = traj["lqL"].shape[1]
+    lqL = np.take_along_axis(traj["lqL"], sel, 1).astype(np.float64)
+    phL = np.take_along_axis(traj["phL"], sel, 1)
+    bh0 = lqL * (2.0 / db) - (np.log(u) / db)[:, None]
+    ck = (np.log(s_nodes) - spec.beta[0]) / db
+    nsec = (spec.nd + 1 + 7) // 8
+    touched = 0
+    for tau in lags:
+        i1 = (sel + int(tau)) % nt
+        lqH = np.take_along_axis(traj["lqH"], i1, 1).astype(np.float64)
+        x3 = (np.take_along_axis(traj["phH"], i1, 1) - phL).astype(np.float64) * (nphi / (2 * np.pi)) % nphi
+        c0 = np.minimum(x3.astype(int), nphi - 1)
+        p = np.where(c0 <= 47, c0, nphi - 1 - c0).ravel()
+        for k in range(s_nodes.size):
+            xb = np.clip(bh0 + ck[k], 0.0, spec.nb - 1 - 1e-6)
+            lqc = lqL + (xb - (bh0 + ck[k])) * (db / 2.0)
+            xd = np.clip((lqH - lqc) / dd - spec.delta[0] / dd, 0.0, spec.nd - 1 - 1e-6)
+            b0, d0 = xb.astype(int).ravel(), xd.astype(int).ravel()
+            bm = np.zeros((48 + 1, spec.nb + 1, nsec + 1), bool)
+            for dp in (0, 1):
+                for db_ in (0, 1):
+                    for dd_ in (0, 1):
+                        bm[p + dp, b0 + db_, (d0 + dd_) // 8] = True
+            touched += int(bm[:49, :spec.nb, :nsec].sum())
+    return 32.0 * touched * (spec.ntau / float(len(lags)))
 
 
 # ----------------------------------------------------------------------------- CPU baseline (oracle port)
@@ -754,8 +811,9 @@ def run_b200(args):
     bytes_per_launch = (32.0 * tm["node_taps"] + 16.0 * tm["tlw_taps"]) / max(launches, 1)
     peak, peak_kind = measured_peaks()
     achieved = bytes_per_launch / (g_ms / 1000.0) / 1e9
-    full = args.templates == N_TEMPLATES and args.nodes == 53 and args.lags == 87
-    traffic = profiled_traffic() if full else None
+    node_taps_launch = tm["node_taps"] / max(launches, 1)
+    traffic, l2_hit, traffic_why = gather_traffic(node_taps_launch)
+    dram_gbs = (traffic / (g_ms / 1000.0) / 1e9) if traffic else None
     line = {"metric": METRIC, "value": value, "unit": "segments/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * dev_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(args),
@@ -769,10 +827,15 @@ def run_b200(args):
             "stages_ms_per_step": {k: tm[k] / args.steps for k in ("filter_ms", "select_ms", "taps_ms", "gather_ms",
                                                                     "epilogue_ms")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "kernel": "k_gather_planes", "peak_kind": peak_kind,
+                         "achieved_is": "logical gather bytes (32 B per node-tap + 16 B of trajectory per tap) per "
+                                        "launch / CUDA-event launch time; served from shared memory, not DRAM",
+                         "traffic": traffic, "traffic_is": "ncu dram read + write bytes per node-tap of a reduced "
+                                                           "case x this launch's node-taps" if traffic else traffic_why,
+                         "achieved_dram": dram_gbs, "frac_dram": (dram_gbs / peak) if dram_gbs else None,
+                         "l2_read_hit_rate": l2_hit,
+                         "kernel": "k_gather_planes", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": g_ms,
-                         "node_taps_per_launch": tm["node_taps"] / max(launches, 1),
-                         "dram_gbs": (traffic / (g_ms / 1000.0) / 1e9) if traffic else None},
+                         "node_taps_per_launch": node_taps_launch},
             "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
@@ -804,6 +867,24 @@ def run_b200(args):
                                           "times), float64 C gather, %.1f s" % (n_t, N_TEMPLATES, t_cpu)}
         line["parity"] = {"templates": n_t, "max_abs_dlnlambda": float(np.abs(lnl_gpu - lnl_cpu).max()),
                           "sample_dlnB": float(abs(restate.log_mean(lnl_gpu, cell) - restate.log_mean(lnl_cpu, cell)))}
+        if args.templates == N_TEMPLATES and args.nodes == 53 and args.lags == 87:
+            # the DRAM floor of the gather: table sectors a 64-template sample touches (5 lags, scaled), plus the
+            # trajectories read once (2 detectors x nm x n_time x 8 B)
+            t0c = time.perf_counter()
+            sub = idx[:64]
+            s1 = restate.read_segments(seg, rows=[args.warmup])
+            traj = restate.trajectories(bank.W[sub], {I: s1["d_" + I][0] for I in "HL"},
+                                        {I: s1["sig2_" + I] for I in "HL"}, bank.lo, bank.n_time, "ref")
+            sel, _ = restate.select_times(traj, spec.tau_idx, N_LOUD, N_RANDOM, 0, bank_rows=sub,
+                                          n_bank=rows.shape[0])
+            lags = spec.tau_idx[np.linspace(0, spec.ntau - 1, 5).astype(int)]
+            comp = compulsory_table_bytes(traj, sel, bank.u[sub], spec, s_nodes, lags)
+            comp += 2.0 * rows.shape[0] * bank.n_time * 8
+            rl = line["roofline"]
+            rl["compulsory_bytes_per_launch_lower_bound"] = comp
+            rl["compulsory_is"] = ("distinct 32-B table sectors touched by a 64-template sample (5 of 87 lags, "
+                                   "scaled) + trajectories once; %.1f s on the host" % (time.perf_counter() - t0c))
+            rl["dram_floor_ms"] = comp / (peak * 1e9) * 1e3
         if args.prec_templates > 0:
             cfg = (ctx.gather_cfg if ctx.gather_cfg is not None else 0, ctx.gather_chunk_pct)
             line["precision"] = precision_legs(args, spec, s_nodes, rows, bank, store, store_h, cfg, local)

@@ -14,10 +14,11 @@ SOURCES = ("gather_fp64.c", "gen_tables.c", "npexp.c")
 
 def build(force=False):
     srcs = [os.path.join(HERE, s) for s in SOURCES]
-    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(s) for s in srcs):
+    deps = srcs + [os.path.abspath(__file__)]    # a change of the flags below rebuilds too
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(s) for s in deps):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-shared", "-fPIC", "-o", OUT] + srcs +
+    subprocess.check_call(["gcc", "-O3", "-ffp-contract=off", "-fopenmp", "-shared", "-fPIC", "-o", OUT] + srcs +
                           ["-lm"])
     return OUT
 
