@@ -25,7 +25,8 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timi
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
-           "exm_redshift_grid", "exm_source_frame", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
+           "exm_redshift_grid", "exm_source_frame", "exm_serve_start", "exm_serve_add_bank", "exm_submit", "exm_poll",
+           "exm_serve_stats", "exm_serve_stop", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -78,6 +79,12 @@ def load():
         "exm_autotune": ([P, I, I, I, P, P, P], I),
         "exm_set_gather_cfg": ([P, I, I], I),
         "exm_redshift_grid": ([P, I, I, P, P, I, P, P, I, P, P], I),
+        "exm_serve_start": ([P, Z, I, I, I, I], I),
+        "exm_serve_add_bank": ([P, I, I, I, I, P, P, P, P, P, D, I, P, P, I, P], I),
+        "exm_submit": ([P, I, P, P, P, P, ctypes.c_int64, P], I),
+        "exm_poll": ([P, ctypes.c_int64, ctypes.c_int64, P, P], I),
+        "exm_serve_stats": ([P, P], I),
+        "exm_serve_stop": ([P], I),
         "exm_source_frame": ([P, P, P, P], I),
         "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
         "exm_store_set_shard": ([P, D], I),
@@ -381,6 +388,58 @@ class Context:
         out = np.empty((ns, nsel), np.float64)
         self._check(self.lib.exm_gather(self.h, nsel, ns, _p(ids), _p(lna), _p(tab), _p(out)))
         return out
+
+    # ---------------------------------------------------------------- native request loop
+
+    def serve_start(self, hbm_budget=0, max_workers=4, n_loud=1024, n_random=1024, graph=False):
+        self._check(self.lib.exm_serve_start(self.h, int(hbm_budget), int(max_workers), int(n_loud), int(n_random),
+                                             1 if graph else 0))
+
+    def serve_add_bank(self, W, lo, n_time, u, M, q, chi, ymin=0.1267, density=None):
+        """register a bank (W (nm, nfreq) complex64); returns its id"""
+        W = np.ascontiguousarray(W, np.complex64)
+        u, M, q, chi = (np.ascontiguousarray(x, np.float64) for x in (u, M, q, chi))
+        bid = ctypes.c_int()
+        if density is None:
+            lny = p = None
+            prior, nd = PRIOR_VOLUME, 0
+        else:
+            lny, p = (np.ascontiguousarray(x, np.float64) for x in density)
+            prior, nd = PRIOR_TABULATED, lny.size
+        self._check(self.lib.exm_serve_add_bank(self.h, W.shape[0], W.shape[1], int(lo), int(n_time), _p(W), _p(u),
+                                                _p(M), _p(q), _p(chi), float(ymin), prior, _p(lny), _p(p), nd,
+                                                ctypes.byref(bid)))
+        return bid.value
+
+    def submit(self, bank_id, d_H, d_L, sig2_H, sig2_L, seed):
+        """queue one segment; returns its handle at once"""
+        d_H, d_L = (np.ascontiguousarray(x, np.complex128) for x in (d_H, d_L))
+        sig2_H, sig2_L = (np.ascontiguousarray(x, np.float64) for x in (sig2_H, sig2_L))
+        h = ctypes.c_int64()
+        self._check(self.lib.exm_submit(self.h, int(bank_id), _p(d_H), _p(d_L), _p(sig2_H), _p(sig2_L), int(seed),
+                                        ctypes.byref(h)))
+        return h.value
+
+    def poll(self, handle, nm, timeout_us=-1):
+        """(ln_lambda (nm,), ln_b) of a finished request, or None if it has not finished within timeout_us"""
+        lnl = np.empty(int(nm), np.float64)
+        lnb = ctypes.c_double()
+        rc = self.lib.exm_poll(self.h, int(handle), int(timeout_us), _p(lnl), ctypes.byref(lnb))
+        if rc == EXM_ERR_TIMEOUT:
+            return None
+        self._check(rc)
+        return lnl, lnb.value
+
+    SERVE_STATS = ("served", "failed", "queued", "running", "workers", "workers_opened", "workers_closed",
+                   "bytes_in_use", "budget", "busy_seconds")
+
+    def serve_stats(self):
+        out = np.zeros(len(self.SERVE_STATS), np.float64)
+        self._check(self.lib.exm_serve_stats(self.h, _p(out)))
+        return dict(zip(self.SERVE_STATS, out.tolist()))
+
+    def serve_stop(self):
+        self._check(self.lib.exm_serve_stop(self.h))
 
     def gather_noalloc(self, nm, n_time, lqH, phH, lqL, phL, nwalk, sel, lw, nsel, ns, mass_ids, lna, tab_ids, out):
         """exm_gather_noalloc: every argument after n_time is a device address (int) the caller owns;

@@ -22,6 +22,7 @@ void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, in
 void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
 void exm_run_np_exp32(exm_ctx *ctx, const float *d_x, float *d_y, long long n);
 void exm_noalloc_load(int dev);
+void exm_serve_destroy(exm_ctx *ctx);
 
 // ------------------------------------------------------------------ memory
 
@@ -411,6 +412,7 @@ static std::mutex g_destroy_mu;   // orders a parent's deferred free against its
 extern "C" void exm_ctx_destroy(exm_ctx *ctx)
 {
     if (!ctx) return;
+    if (ctx->srv) exm_serve_destroy(ctx);   // its workers are children of this context
     exm_ctx *parent = ctx->parent, *free_parent = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_destroy_mu);

@@ -44,6 +44,7 @@ struct exm_error {
 // ------------------------------------------------------------------ device buffers
 
 struct exm_ctx;
+struct exm_server;   // the native request loop of a context (serve.cu)
 
 struct dbuf {
     void *p = nullptr;
@@ -130,7 +131,8 @@ struct exm_ctx {
     struct exm_redshift *rs = nullptr;   // pe_redshift's grid and buffers (csrc/redshift.cu)
     int gather_cfg = 0;
     int gather_chunk_pct = 100;
-    bool test_wait_expiry = false;   // the plane gather stages nothing and its barrier waits run out (a test)   // templates per gather block, percent of the one-wave-per-lag size
+    bool test_wait_expiry = false;
+    exm_server *srv = nullptr;       // request loop served from this context (exm_serve_start)   // the plane gather stages nothing and its barrier waits run out (a test)   // templates per gather block, percent of the one-wave-per-lag size
 
     // cuFFT
     cufftHandle plan = 0;

@@ -249,6 +249,52 @@ EXM_API int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *
  * templates per gather block in percent of the default (10..1000; 0 keeps the current). */
 EXM_API int exm_set_gather_cfg(exm_ctx *ctx, int cfg, int chunk_pct);
 
+/* ------------------------------------------------------------------ serving (native request loop) */
+
+/* Start a request loop on ctx, the context that owns the resident store.  The reference analyses one
+ * pe_intrinsic call at a time (exmarg/search/pe.py:289-346); this loop admits requests continuously:
+ * workers are child contexts (exm_ctx_create_sharing) on host threads of their own, each holding one
+ * bank and one workspace, opened and closed within hbm_budget bytes (0: 85% of the free device memory)
+ * and max_workers (1..64).  A request starts on an idle worker of its bank; a bank with no worker may
+ * close idle workers of banks with nothing queued to make room; a bank whose workers are busy waits for
+ * one unless the budget has room for another.  A worker's cost is estimated from its bank's shape until
+ * its first segment has run, then measured.  Every request uses n_loud / n_random (as exm_pe_intrinsic)
+ * and, with use_graph, each worker replays its segments as a captured CUDA graph.  Workers take ctx's
+ * gather launch shape, so a served result is bitwise exm_pe_intrinsic's on ctx for the same bank,
+ * segment and seed, whatever runs beside it.  Requests started while others run get decreasing stream
+ * priorities (the oldest leads). */
+EXM_API int exm_serve_start(exm_ctx *ctx, size_t hbm_budget, int max_workers, int n_loud, int n_random,
+                            int use_graph);
+
+/* Register a bank with the server (before the first request): as exm_bank_set (nm <= 8192) followed
+ * by exm_pe_prepare (ymin, prior, density).  *bank_id receives its id for exm_submit.  Replaces
+ * mass_bank's device state (exmarg/search/bank.py:35-54) held per worker. */
+EXM_API int exm_serve_add_bank(exm_ctx *ctx, int nm, int nfreq, int lo, int n_time, const float *W,
+                               const double *u, const double *M, const double *q, const double *chi, double ymin,
+                               int prior, const double *lny, const double *p_lny, int n_dens, int *bank_id);
+
+/* Queue one segment for bank bank_id and return at once with *handle.  d_H, d_L: (nfreq) complex128
+ * (interleaved), sig2_H, sig2_L: (nfreq) float64 -- copied, so the caller's buffers are free when this
+ * returns; seed: the random-draw seed of the segment (the reference's seed + row).  The equivalent of
+ * one row of pe_intrinsic (exmarg/search/pe.py:289-346).  Safe to call from several host threads. */
+EXM_API int exm_submit(exm_ctx *ctx, int bank_id, const double *d_H, const double *d_L, const double *sig2_H,
+                       const double *sig2_L, int64_t seed, int64_t *handle);
+
+/* Wait up to timeout_us microseconds (0: do not wait; negative: until done) for request `handle`.
+ * EXM_OK: ln_lambda (the bank's nm, float64, bank order) and *ln_b are written and the handle is
+ * released; EXM_ERR_TIMEOUT: not finished yet (poll again); any other status: the request failed
+ * (message in exm_last_error) and the handle is released.  Safe to call from several host threads. */
+EXM_API int exm_poll(exm_ctx *ctx, int64_t handle, int64_t timeout_us, double *ln_lambda, double *ln_b);
+
+/* Server counters, out (10 doubles): requests served, failed, queued, running; workers open, opened in
+ * all, closed for budget; workspace bytes in use (estimated or measured), the budget; seconds from the
+ * first request of an idle server to the last result. */
+EXM_API int exm_serve_stats(exm_ctx *ctx, double *out);
+
+/* Stop the server: running requests finish, queued ones fail, workers close; handles not yet polled
+ * become invalid.  exm_ctx_destroy stops a server that is still running. */
+EXM_API int exm_serve_stop(exm_ctx *ctx);
+
 /* ------------------------------------------------------------------ stages (tests, gather-level drop-in) */
 
 /* Matched filter of one segment (exmarg/search/bank.py:56-78, MassBank.trajectories):
