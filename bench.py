@@ -345,12 +345,19 @@ def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, 
     return out
 
 
-def batched_leg(args, store, bank, local):
-    """the batched workload: n segments with network SNR drawn from U(0, 30), 30 % noise-only, float32
-    strain, analysed by one pe_intrinsic call on a context that replays each segment as a captured CUDA
-    graph (the 2048-template bank and resident store of the main run)"""
+def batched_leg(args, store, bank, local, spec, s_nodes, rows, store_h):
+    """the batched workload: args.batch_segments segments (8 s, float32 strain, network SNR drawn from U(0, 30),
+    30 % noise-only) of the 2048-template bank on the resident store, as
+      graph_replay: one pe_intrinsic call over all of them on a context that replays each segment as a
+        captured CUDA graph (one segment on the device at a time);
+      native_server: all submitted at once to the native request loop (exm_submit / exm_poll) with
+        args.batch_workers workers of the bank, graph replay on each: segments overlap on the device, the
+        oldest one's gather leading by stream priority.
+    Every served ln Lambda is compared with the graph-replay call's (same bank, segment and seed); ln B of a
+    sample of segments is checked against the float64 oracle on a template sample."""
     import exmarg_b200 as eb
     from exmarg_b200 import synth
+    from oracle import restate
     n = args.batch_segments
     segs = synth.make_segments(n + 1, segment_seed(0) + 4242, T=T_SEG, fmax=FMAX, snr=(0.0, 30.0), noise_only=0.3,
                                mc=(10.0, 40.0), q=(0.25, 1.0), chi=(-0.5, 0.5), dtype=np.complex64)
@@ -365,9 +372,41 @@ def batched_leg(args, store, bank, local):
         tm = ctx.timing(False)
     finally:
         ctx.set_graph(False)
-    return {"segments": n, "segments_per_s": n / (tm["total_ms"] / 1000.0), "e2e_segments_per_s": n / wall,
-            "snr": "U(0, 30), 30% noise-only", "strain": "complex64", "graph_replay": True,
-            "ln_b_range": [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]}
+    out = {"segments": n, "snr": "U(0, 30), 30% noise-only", "strain": "complex64",
+           "graph_replay": {"segments_per_s": n / (tm["total_ms"] / 1000.0), "e2e_segments_per_s": n / wall}}
+    # the native request loop, several workers of the one bank
+    rd = eb.read_segments(segs)
+    ctx.serve_start(hbm_budget=0, max_workers=args.batch_workers, n_loud=N_LOUD, n_random=N_RANDOM, graph=True)
+    try:
+        bid = ctx.serve_add_bank(bank.W, bank.lo, bank.n_time, bank.u, bank.M, bank.q, bank.chi, 0.1267)
+        warm = [ctx.submit(bid, rd["d_H"][0], rd["d_L"][0], rd["sig2_H"], rd["sig2_L"], 0)
+                for _ in range(args.batch_workers)]          # opens the workers and captures their graphs
+        for h in warm:
+            ctx.poll(h, bank.u.size)
+        t0 = time.perf_counter()
+        hs = [ctx.submit(bid, rd["d_H"][e], rd["d_L"][e], rd["sig2_H"], rd["sig2_L"], e) for e in range(1, n + 1)]
+        got = [ctx.poll(h, bank.u.size) for h in hs]
+        wall_s = time.perf_counter() - t0
+        st = ctx.serve_stats()
+    finally:
+        ctx.serve_stop()
+    same = all(np.array_equal(g[0], res["ln_lambda"][i]) for i, g in enumerate(got))
+    out["native_server"] = {"workers": args.batch_workers, "segments_per_s": n / wall_s,
+                            "identical_to_plain": bool(same), "workers_opened": st["workers_opened"]}
+    # parity: the float64 oracle on a template sample of a few segments
+    k_seg = min(args.batch_check_segments, n)
+    idx = np.sort(np.random.default_rng(13).choice(rows.shape[0], args.batch_check_templates, replace=False))
+    cell = restate.cell_weights(rows[idx, 0], rows[idx, 1], rows[idx, 2])
+    errs = []
+    for e in np.linspace(1, n, k_seg).astype(int):
+        o = restate.pe_intrinsic(restate.read_segments(segs, rows=[int(e)]), bank.W[idx], bank.u[idx], rows[idx, 0],
+                                 rows[idx, 1], rows[idx, 2], bank.lo, bank.n_time, store_h, n_loud=N_LOUD,
+                                 n_random=N_RANDOM, seed=0, precision="ref", bank_rows=idx, n_bank=rows.shape[0])
+        errs.append(abs(restate.log_mean(res["ln_lambda"][e - 1][idx], cell) - restate.log_mean(o["ln_lambda"][0], cell)))
+    out["parity"] = {"segments_checked": k_seg, "templates": int(idx.size),
+                     "max_abs_dlnB_vs_reference_port": float(max(errs))}
+    out["ln_b_range"] = [float(np.min(res["ln_b"])), float(np.max(res["ln_b"]))]
+    return out
 
 
 def redshift_leg(args, store, seg, local):
@@ -843,8 +882,7 @@ def run_b200(args):
             "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
-    if rank == 0 and world == 1 and args.batch_segments > 0:
-        line["batched"] = batched_leg(args, store, bank, local)
+
     if rank == 0 and world == 1 and args.redshift_segments > 0:
         line["redshift"] = redshift_leg(args, store, seg, local)
     if rank == 0 and world == 1 and args.io_nodes > 0:
@@ -889,6 +927,8 @@ def run_b200(args):
             rl["compulsory_is"] = ("distinct 32-B table sectors touched by a 64-template sample (5 of 87 lags, "
                                    "scaled) + trajectories once; %.1f s on the host" % (time.perf_counter() - t0c))
             rl["dram_floor_ms"] = comp / (peak * 1e9) * 1e3
+        if args.batch_segments > 0:
+            line["batched"] = batched_leg(args, store, bank, local, spec, s_nodes, rows, store_h)
         if args.prec_templates > 0:
             cfg = (ctx.gather_cfg if ctx.gather_cfg is not None else 0, ctx.gather_chunk_pct)
             line["precision"] = precision_legs(args, spec, s_nodes, rows, bank, store, store_h, cfg, local)
@@ -929,7 +969,10 @@ def main():
     ap.add_argument("--io-readers", type=int, default=6, help="reader threads of the store-loading leg")
     ap.add_argument("--io-dir", default=None, help="where the store-loading leg writes its files (default: TMPDIR)")
     ap.add_argument("--redshift-segments", type=int, default=8, help="segments of the pe_redshift leg (0: none)")
-    ap.add_argument("--batch-segments", type=int, default=16, help="segments of the batched leg (0: none)")
+    ap.add_argument("--batch-segments", type=int, default=256, help="segments of the batched leg (0: none)")
+    ap.add_argument("--batch-workers", type=int, default=3, help="native-server workers of the batched leg")
+    ap.add_argument("--batch-check-segments", type=int, default=4, help="batched segments checked by the oracle")
+    ap.add_argument("--batch-check-templates", type=int, default=32, help="templates of that oracle check")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
     ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
     args = ap.parse_args()

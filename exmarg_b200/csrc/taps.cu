@@ -357,9 +357,14 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           exm_dtype_wd(ctx->dtype), exm_dtype_calign(ctx->dtype), (int *)sl.win.p);
     k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
-    const long long n_chunks = (long long)rc * a.pitch / EXM_DCH;
-    k_tap_interleave<<<(int)std::min<long long>(n_chunks, (long long)ctx->sm_count * 32), 256, 0, ctx->stream>>>(
-        a.desc, a.tside, n_chunks);
+    // k_gather_planes reads lane-interleaved chunks, k_gather_runs the sorted order as scattered
+    sl.desc_sorted = exm_gather_cfg_sorted(ctx->gather_cfg);
+    if (!sl.desc_sorted) {
+        const long long n_chunks = (long long)rc * a.pitch / EXM_DCH;
+        k_tap_interleave<<<(int)std::min<long long>(n_chunks, (long long)ctx->sm_count * 32), 256, 0,
+                           ctx->stream>>>(a.desc, a.tside, n_chunks);
+        ctx->launches += 1;
+    }
     EXM_CUDA(cudaGetLastError());
-    ctx->launches += 5;
+    ctx->launches += 4;
 }
