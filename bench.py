@@ -787,6 +787,98 @@ def serving_legs(args, store, bank, seg, rows, plain, capacity, local):
     return out
 
 
+SERVE_BANKS = (("b256_4s", 256, 4.0), ("b256_16s", 256, 16.0), ("b2048_8s", 2048, 8.0), ("b2048_16s", 2048, 16.0),
+               ("b8192_4s", 8192, 4.0), ("b8192_8s", 8192, 8.0))
+
+
+def serve_config_leg(args, store, local):
+    """The serving workload through the native request loop (exm_submit / exm_poll): banks of 256, 2048 and 8192
+    TaylorF2 templates on 4, 8 and 16 s segments (SERVE_BANKS; 2048 Hz strain, 20-512 Hz analysed), segments
+    with network SNR U(0, 50) and 90 % noise-only, the 53-node store resident, workers opened and closed within
+    the HBM budget.  First args.serve_capacity_requests requests are queued at once: their rate is the mixed
+    capacity.  Then args.serve_poisson_requests arrive as a Poisson stream at args.serve_load x that capacity
+    (the config's 400 req/s is stated beside it as a multiple of the capacity).  Latency is arrival to result
+    (p50 / p99); a sample of served results is compared bitwise with the plain single-segment path."""
+    import exmarg_b200 as eb
+    from exmarg_b200 import synth
+    ctx = eb.context(local)
+    rng = np.random.default_rng(2027)
+    banks, segs = {}, {}
+    for key, nm, T in SERVE_BANKS:
+        sg = synth.make_segments(16, segment_seed(0) + int(T * 1000) + nm, T=T, fmax=FMAX, snr=(0.0, 50.0),
+                                 noise_only=0.9, mc=(10.0, 40.0), q=(0.25, 1.0), chi=(-0.5, 0.5))
+        rows = synth.make_bank(nm, BANK_SEED + nm)
+        banks[key] = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], sg, "b200", device_index=local)
+        segs[key] = eb.read_segments(sg)
+    keys = [k for k, _, _ in SERVE_BANKS]
+    weights = np.array([0.2, 0.2, 0.2, 0.15, 0.15, 0.1])
+    n_cap, n_poi = args.serve_capacity_requests, args.serve_poisson_requests
+    mix = [(keys[int(rng.choice(len(keys), p=weights))], int(rng.integers(0, 16))) for _ in range(n_cap + n_poi)]
+    free0, total0 = eb.device_memory(local)
+    ctx.serve_start(hbm_budget=0, max_workers=args.serve_workers, n_loud=N_LOUD, n_random=N_RANDOM, graph=True)
+    out = {"banks": {k: {"templates": nm, "segment_s": T} for k, nm, T in SERVE_BANKS},
+           "mix_weights": weights.tolist(), "snr": "U(0, 50), 90% noise-only", "workers_max": args.serve_workers}
+    try:
+        ids = {k: ctx.serve_add_bank(b.W, b.lo, b.n_time, b.u, b.M, b.q, b.chi, 0.1267) for k, b in banks.items()}
+        stats0 = ctx.serve_stats()
+        out["hbm_budget_gb"] = stats0["budget"] / 1e9
+
+        def submit(key, e):
+            sg = segs[key]
+            return ctx.submit(ids[key], sg["d_H"][e], sg["d_L"][e], sg["sig2_H"], sg["sig2_L"], e)
+
+        # warm-up: one request per bank (opens workers, plans, graphs)
+        for k in keys:
+            ctx.poll(submit(k, 0), banks[k].u.size)
+        # capacity: everything queued at once
+        t0 = time.perf_counter()
+        hs = [(submit(k, e), k, e) for k, e in mix[:n_cap]]
+        served = [(ctx.poll(h, banks[k].u.size), k, e) for h, k, e in hs]
+        cap = n_cap / (time.perf_counter() - t0)
+        out["capacity"] = {"requests": n_cap, "segments_per_s": cap}
+        # the Poisson stream at a stated fraction of that capacity
+        rate = args.serve_load * cap
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_poi))
+        pend, lat, done_t = {}, [], []
+        t0 = time.perf_counter()
+        i = 0
+        while i < n_poi or pend:
+            now = time.perf_counter() - t0
+            while i < n_poi and arrivals[i] <= now:
+                k, e = mix[n_cap + i]
+                pend[submit(k, e)] = (k, arrivals[i])
+                i += 1
+            for h in list(pend):
+                k, ta = pend[h]
+                r = ctx.poll(h, banks[k].u.size, timeout_us=0)
+                if r is not None:
+                    tn = time.perf_counter() - t0
+                    lat.append(tn - ta)
+                    done_t.append(tn)
+                    del pend[h]
+            time.sleep(0.0005)
+        st = ctx.serve_stats()
+        lat = np.array(lat)
+        out["poisson"] = {"requests": n_poi, "offered_per_s": rate, "offered_fraction_of_capacity": args.serve_load,
+                          "segments_per_s": n_poi / (max(done_t) - arrivals[0]),
+                          "latency_ms_p50": float(np.percentile(lat, 50) * 1e3),
+                          "latency_ms_p99": float(np.percentile(lat, 99) * 1e3),
+                          "config_rate_400_per_s_as_multiple_of_capacity": 400.0 / cap}
+        out["workers_opened"], out["workers_closed_for_budget"] = st["workers_opened"], st["workers_closed"]
+        out["failed"] = st["failed"]
+    finally:
+        ctx.serve_stop()
+    # bitwise check of served results against the plain path on the parent context (a sample)
+    same, checked = True, 0
+    for (lnl, lnb), k, e in served[:: max(1, len(served) // 12)]:
+        r = eb.pe_intrinsic(segs[k], banks[k], store, rows=[e], seed=0)
+        same &= bool(np.array_equal(r["ln_lambda"][0], lnl)) and float(r["ln_b"][0]) == lnb
+        checked += 1
+    out["identical_to_plain"] = {"checked": checked, "bitwise": same}
+    out["device_memory_gb"] = {"free_at_start": free0 / 1e9, "total": total0 / 1e9}
+    return out
+
+
 def run_b200(args):
     rank, world, local = dist_env()
     import exmarg_b200 as eb
@@ -880,6 +972,8 @@ def run_b200(args):
                          "algorithmic_bytes_per_launch": bytes_per_launch, "launch_ms": g_ms,
                          "node_taps_per_launch": node_taps_launch},
             "gather_gbs_logical": achieved, "clocks": clk, "autotune": tune}
+    if rank == 0 and world == 1 and args.serve_config:
+        line["serving_config"] = serve_config_leg(args, store, local)
     if rank == 0 and world == 1 and args.serve_requests > 0:
         line["serving"] = serving_legs(args, store, bank, seg, rows, res, value, local)
 
@@ -975,6 +1069,11 @@ def main():
     ap.add_argument("--batch-check-templates", type=int, default=32, help="templates of that oracle check")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of each serving leg (0: none)")
     ap.add_argument("--serve-workers", type=int, default=3, help="serving workers (child contexts)")
+    ap.add_argument("--serve-config", action="store_true",
+                    help="the serving workload at its stated shape through the native request loop (minutes)")
+    ap.add_argument("--serve-capacity-requests", type=int, default=200, help="requests queued at once (capacity)")
+    ap.add_argument("--serve-poisson-requests", type=int, default=1000, help="requests of the Poisson stream")
+    ap.add_argument("--serve-load", type=float, default=0.8, help="Poisson rate as a fraction of the capacity")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
