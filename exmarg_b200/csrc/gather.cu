@@ -854,18 +854,20 @@ __device__ __forceinline__ void runs_pass(const PlaneArgs &a, const RunsCtx &c, 
         const bool fin = active && npos == end;
         int npos2 = npos;
         if (__any_sync(0xffffffffu, fin)) {
-            // the group's lanes hold partials of one template: combine them, the first lane keeps the total
+            // a finishing group's lanes hold partials of one template: combine them in copies (the lanes of
+            // groups still inside a run keep their own partials), the first lane merges the total
+            float tB = cB, tE = cE, tS = cS;
 #pragma unroll
             for (int o = EXM_RG / 2; o > 0; o >>= 1) {
-                const float B2 = __shfl_xor_sync(0xffffffffu, cB, o);
-                const float E2 = __shfl_xor_sync(0xffffffffu, cE, o);
-                const float S2 = __shfl_xor_sync(0xffffffffu, cS, o);
-                lse_merge(cB, cE, cS, B2, E2, S2);
+                const float B2 = __shfl_xor_sync(0xffffffffu, tB, o);
+                const float E2 = __shfl_xor_sync(0xffffffffu, tE, o);
+                const float S2 = __shfl_xor_sync(0xffffffffu, tS, o);
+                lse_merge(tB, tE, tS, B2, E2, S2);
             }
             if (fin) {
-                if (gl == 0 && cS > 0.f) {
+                if (gl == 0 && tS > 0.f) {
                     float b = accB[j], x = accE[j], s = accS[j];
-                    lse_merge(b, x, s, cB, cE, cS);
+                    lse_merge(b, x, s, tB, tE, tS);
                     accB[j] = b;
                     accE[j] = x;
                     accS[j] = s;
