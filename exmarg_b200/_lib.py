@@ -16,13 +16,14 @@ LIB_PATH = os.path.join(HERE, "libexmarg_b200.so")
 EXM_OK, EXM_ERR_ARG, EXM_ERR_OOM, EXM_ERR_CUDA, EXM_ERR_TIMEOUT, EXM_ERR_STATE = range(6)
 DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
+QUAD_GL64 = 16   # OR'ed into the prior: 64-point Gauss-Legendre distance quadrature
 # the plane gather's launch shapes, in exm_autotune / exm_set_gather_cfg order: k_gather_planes (warps per
 # block x taps per register group), then k_gather_runs (warps per block)
 GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2",
                  "runs 16w", "runs 20w", "runs 24w")
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_rng_integers", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
@@ -53,6 +54,7 @@ def load():
         "exm_version": ([], I),
         "exm_device_memory": ([I, ctypes.POINTER(Z), ctypes.POINTER(Z)], I),
         "exm_rng_integers": ([ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int64, P], I),
+        "exm_gauss_legendre": ([I, P, P], I),
         "exm_ctx_create": ([I, Z, ctypes.POINTER(P)], I),
         "exm_ctx_destroy": ([P], None),
         "exm_ctx_create_sharing": ([P, Z, ctypes.POINTER(P)], I),
@@ -108,6 +110,15 @@ def rng_integers(seed, high, count):
     if rc != EXM_OK:
         _raise(rc, "bad rng arguments")
     return out
+
+
+def gauss_legendre(n):
+    """the n-point Gauss-Legendre nodes and weights on [-1, 1], by the library's host code"""
+    x, w = np.empty(int(n)), np.empty(int(n))
+    rc = load().exm_gauss_legendre(int(n), _p(x), _p(w))
+    if rc != EXM_OK:
+        _raise(rc, "n must be 1..256")
+    return x, w
 
 
 def device_memory(device=0):
@@ -319,13 +330,14 @@ class Context:
         self.nm, self.nfreq, self.n_time = nm, nf, int(n_time)
         self.prep_token = None
 
-    def prepare(self, ymin, prior, density=None):
+    def prepare(self, ymin, prior, density=None, gl64=False):
+        q = QUAD_GL64 if gl64 else 0
         if prior == PRIOR_TABULATED:
             lny = np.ascontiguousarray(density[0], np.float64)
             p = np.ascontiguousarray(density[1], np.float64)
-            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), prior, _p(lny), _p(p), lny.size))
+            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), prior | q, _p(lny), _p(p), lny.size))
         else:
-            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), PRIOR_VOLUME, None, None, 0))
+            self._check(self.lib.exm_pe_prepare(self.h, float(ymin), PRIOR_VOLUME | q, None, None, 0))
 
     # analysis -------------------------------------------------------------
     def pe_intrinsic(self, d_H, d_L, sig2_H, sig2_L, seeds, n_loud, n_random):

@@ -18,7 +18,7 @@ void exm_make_tmap(exm_ctx *ctx);
 void exm_store_generate(exm_ctx *ctx, int k, const float *M, const float *P, const float *Q, float S, uint32_t seed);
 void exm_run_node_values(exm_ctx *ctx, exm_slot &sl, double *d_lamN);
 void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,
-                                const double *d_p, int n_dens);
+                                const double *d_p, int n_dens, const double *d_gl);
 void exm_run_topk(exm_ctx *ctx, exm_slot &sl, int nmc, const int *d_order_chunk, int K, int S);
 void exm_run_np_exp32(exm_ctx *ctx, const float *d_x, float *d_y, long long n);
 void exm_noalloc_load(int dev);
@@ -660,12 +660,56 @@ static void upload(exm_ctx *ctx, dbuf &b, const std::vector<T> &v)
     if (!v.empty()) EXM_CUDA(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
 }
 
+// The n-point Gauss-Legendre rule on [-1, 1]: the nodes are the roots of the Legendre polynomial P_n, found by
+// Newton's method from the asymptotic guesses cos(pi (i + 3/4) / (n + 1/2)) with P_n and P_n' from the
+// three-term recurrence (k + 1) P_{k+1} = (2k + 1) x P_k - k P_{k-1}; the weights are 2 / ((1 - x^2) P_n'(x)^2).
+// Symmetric pairs are computed once.
+void exm_gauss_legendre_rule(int n, double *x, double *w)
+{
+    const double pi = 3.14159265358979323846;
+    for (int i = 0; i < (n + 1) / 2; ++i) {
+        double z = std::cos(pi * (i + 0.75) / (n + 0.5)), dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 1; k < n; ++k) {
+                const double p2 = ((2.0 * k + 1.0) * z * p1 - k * p0) / (k + 1.0);
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1.0);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) < 1e-16) break;
+        }
+        double p0 = 1.0, p1 = z;
+        for (int k = 1; k < n; ++k) {
+            const double p2 = ((2.0 * k + 1.0) * z * p1 - k * p0) / (k + 1.0);
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = n * (z * p1 - p0) / (z * z - 1.0);
+        const double wi = 2.0 / ((1.0 - z * z) * dp * dp);
+        x[n - 1 - i] = z;
+        x[i] = -z;
+        w[i] = w[n - 1 - i] = wi;
+    }
+}
+
+extern "C" int exm_gauss_legendre(int n, double *x, double *w)
+{
+    if (n < 1 || n > 256 || !x || !w) return EXM_ERR_ARG;
+    exm_gauss_legendre_rule(n, x, w);
+    return EXM_OK;
+}
+
 extern "C" int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double *lny, const double *p_lny, int n_dens)
 {
     API_BEGIN(ctx)
     EXM_CUDA(cudaSetDevice(ctx->dev));
     REQUIRE(ctx->store_ok, EXM_ERR_STATE, "store is not complete (exm_store_init + every node)");
     REQUIRE(ctx->bank_ok, EXM_ERR_STATE, "no bank (exm_bank_set)");
+    const bool gl64 = (prior & EXM_QUAD_GL64) != 0;
+    prior &= ~EXM_QUAD_GL64;
     REQUIRE(prior == EXM_PRIOR_VOLUME || (prior == EXM_PRIOR_TABULATED && lny && p_lny && n_dens >= 2), EXM_ERR_ARG,
             "the distance prior is 'volume' or a tabulated density");
     const int nn = ctx->nn, nm = ctx->nm;
@@ -767,12 +811,20 @@ extern "C" int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double
         dens.insert(dens.end(), p_lny, p_lny + n_dens);
     }
     upload(ctx, dd, dens);
+    dbuf dg;
+    if (gl64) {
+        std::vector<double> g(128);
+        exm_gauss_legendre_rule(64, g.data(), g.data() + 64);
+        upload(ctx, dg, g);
+    }
     exm_ensure(ctx, ctx->d_lnW, sizeof(double) * (size_t)(nn + 1) * nm);
     exm_run_distance_weights_y(ctx, (const double *)dy.p, ymin, prior, (const double *)dd.p,
-                               (const double *)dd.p + (dens.empty() ? 0 : n_dens), n_dens);
+                               (const double *)dd.p + (dens.empty() ? 0 : n_dens), n_dens,
+                               gl64 ? (const double *)dg.p : nullptr);
     EXM_CUDA(cudaStreamSynchronize(ctx->stream));
     exm_free(ctx, dy);
     exm_free(ctx, dd);
+    exm_free(ctx, dg);
     ctx->prep_ok = true;
     ctx->traj_ok = ctx->times_ok = false;
     API_END(ctx)

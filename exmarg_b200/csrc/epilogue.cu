@@ -26,10 +26,12 @@ __device__ double interp_density(double t, const double *xp, const double *fp, i
     return slope * (t - xp[lo]) + fp[lo];
 }
 
-// y (nn + 1, nm): the template's points (0 where none), internal order; lnW out
+// y (nn + 1, nm): the template's points (0 where none), internal order; lnW out.  gl (2 x 64: nodes, weights
+// on [-1, 1]) non-null: every interval by 64-point Gauss-Legendre in x = ln y, p(x) (b - x) / h and
+// p(x) (x - a) / h with p the volume density 3 ymin^3 e^{-3x} or the tabulated one
 __global__ void k_distance_weights(const double *__restrict__ y, int nn1, int nm, double ymin, int prior,
                                    const double *__restrict__ lny, const double *__restrict__ plny, int n_dens,
-                                   double *__restrict__ lnW)
+                                   const double *__restrict__ gl, double *__restrict__ lnW)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nm) return;
@@ -54,7 +56,18 @@ __global__ void k_distance_weights(const double *__restrict__ y, int nn1, int nm
     for (int j = 0; j + 1 < np_; ++j) {
         const double a = log(yy[j]), b = log(yy[j + 1]);
         const double h = b - a;
-        if (prior == EXM_PRIOR_VOLUME) {
+        if (gl) {
+            const double c = 3.0 * ymin * ymin * ymin, mid = 0.5 * (a + b), half = 0.5 * h;
+            double s0 = 0.0, s1 = 0.0;
+            for (int q = 0; q < 64; ++q) {
+                const double t = mid + half * gl[q];
+                const double f = (prior == EXM_PRIOR_VOLUME) ? c * exp(-3.0 * t) : interp_density(t, lny, plny, n_dens);
+                s0 += gl[64 + q] * f * (b - t);
+                s1 += gl[64 + q] * f * (t - a);
+            }
+            w[j] += s0 * half / h;
+            w[j + 1] += s1 * half / h;
+        } else if (prior == EXM_PRIOR_VOLUME) {
             const double c = 3.0 * ymin * ymin * ymin, kk = 3.0;
             const double ea = exp(-kk * a), eb = exp(-kk * b);
             const double I0 = (ea - eb) / kk;
@@ -177,9 +190,9 @@ void exm_run_lnb(exm_ctx *ctx, exm_slot &sl)
 }
 
 void exm_run_distance_weights_y(exm_ctx *ctx, const double *d_y, double ymin, int prior, const double *d_lny,
-                                const double *d_p, int n_dens)
+                                const double *d_p, int n_dens, const double *d_gl)
 {
     k_distance_weights<<<(ctx->nm + 127) / 128, 128, 0, ctx->stream>>>(d_y, ctx->nn + 1, ctx->nm, ymin, prior, d_lny,
-                                                                       d_p, n_dens, (double *)ctx->d_lnW.p);
+                                                                       d_p, n_dens, d_gl, (double *)ctx->d_lnW.p);
     EXM_CUDA(cudaGetLastError());
 }

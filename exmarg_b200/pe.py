@@ -27,26 +27,37 @@ def _density_key(prior):
     return ("tabulated", a.size, hash(a.tobytes()), hash(b.tobytes()))
 
 
-def prepare(bank, store, prior="volume", ymin=0.1267):
+QUADRATURES = ("reference", "gl64")
+
+
+def prepare(bank, store, prior="volume", ymin=0.1267, quadrature="reference"):
     """make (store, bank, prior, ymin) current on the bank's context: tables resident, geometry and
-    distance weights computed on the device (once; later calls with the same inputs reuse them)"""
+    distance weights computed on the device (once; later calls with the same inputs reuse them).
+    quadrature: 'reference' integrates the distance prior as exmarg/search/pe.py:260-286 does (closed form
+    for the volume prior, 401-point trapezoid per interval for a tabulated density); 'gl64' uses 64-point
+    Gauss-Legendre in ln y on every interval for both"""
+    if quadrature not in QUADRATURES:
+        raise ValueError("quadrature must be 'reference' or 'gl64'")
     ctx = bank.ctx
     upload_store(store, ctx)
     bank.upload()
-    key = (ctx.store_token, ctx.bank_token, prior if isinstance(prior, str) else _density_key(prior), float(ymin))
+    key = (ctx.store_token, ctx.bank_token, prior if isinstance(prior, str) else _density_key(prior), float(ymin),
+           quadrature)
     if ctx.prep_token != key:
         density = distance_density(prior)
+        gl = quadrature == "gl64"
         if density is None:
-            ctx.prepare(ymin, _lib.PRIOR_VOLUME)
+            ctx.prepare(ymin, _lib.PRIOR_VOLUME, gl64=gl)
         else:
-            ctx.prepare(ymin, _lib.PRIOR_TABULATED, density)
+            ctx.prepare(ymin, _lib.PRIOR_TABULATED, density, gl64=gl)
         ctx.prep_token = key
     return ctx
 
 
 def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, chunk=4, nodes_per_launch=6,
-                 block=256, resident=False, n_loud=1024, n_random=1024, seed=0):
+                 block=256, resident=False, n_loud=1024, n_random=1024, seed=0, quadrature="reference"):
     """ln Lambda of each template of the bank, the distance integrated over its prior.
+    quadrature ('b200' only): 'reference' (the reference's rules) or 'gl64' (see prepare).
 
     returns dict: M, q, chi, u (n_template,), ln_lambda (n_segment, n_template),
     ln_b (n_segment,), rows."""
@@ -60,7 +71,7 @@ def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, 
     if int(nodes_per_launch) < 1 or int(chunk) < 1:
         raise ValueError("chunk and nodes_per_launch must be >= 1")
     seg = read_segments(segments, rows)
-    ctx = prepare(bank, store, prior, ymin)
+    ctx = prepare(bank, store, prior, ymin, quadrature)
     seeds = seed + np.asarray(seg["rows"], np.int64)
     apply_tuned(ctx, n_loud, n_random)
     lnl, lnb = ctx.pe_intrinsic(seg["d_H"], seg["d_L"], seg["sig2_H"], seg["sig2_L"], seeds, n_loud, n_random)

@@ -41,6 +41,8 @@ extern "C" {
 
 #define EXM_PRIOR_VOLUME 0
 #define EXM_PRIOR_TABULATED 1 /* a density of ln y on a grid ('madau-dickinson') */
+#define EXM_QUAD_GL64 16      /* OR'ed into the prior: 64-point Gauss-Legendre on every interval between
+                                 a template's node points, in place of the reference's rules */
 
 typedef struct exm_ctx exm_ctx;
 
@@ -218,10 +220,18 @@ EXM_API int exm_bank_set(exm_ctx *ctx, int nm, int nfreq, int lo, int n_time, co
  * (pe.py:260-286 and :321-327, computed on the device in float64) and cell
  * weights (pe.py:338-343) for the current store and bank.  prior
  * EXM_PRIOR_VOLUME, or EXM_PRIOR_TABULATED with the density (lny, p_lny) of
- * n_dens points ('madau-dickinson', exmarg/priors.py:31-38).  Fails with
+ * n_dens points ('madau-dickinson', exmarg/priors.py:31-38); | EXM_QUAD_GL64
+ * integrates every interval with 64 Gauss-Legendre points in ln y instead of the
+ * reference's closed form (volume) or 401-point trapezoid (tabulated).  Fails with
  * EXM_ERR_ARG and the reference's message when a template reaches fewer than
  * two nodes (pe.py:324-325). */
 EXM_API int exm_pe_prepare(exm_ctx *ctx, double ymin, int prior, const double *lny, const double *p_lny, int n_dens);
+
+/* The n-point Gauss-Legendre rule on [-1, 1] (n <= 256), nodes x (ascending) and weights w, float64, by Newton
+ * iteration on the Legendre recurrence: the rule exm_pe_prepare uses with EXM_QUAD_GL64 (64 points).  No GPU
+ * needed.  No reference counterpart (the reference integrates in closed form or by the trapezoid rule,
+ * exmarg/search/pe.py:260-286). */
+EXM_API int exm_gauss_legendre(int n, double *x, double *w);
 
 /* pe_intrinsic on n_seg segments (exmarg/search/pe.py:289-346): d_H, d_L
  * (n_seg, nfreq) complex128 (interleaved), sig2_H, sig2_L (nfreq) float64,

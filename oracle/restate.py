@@ -209,16 +209,24 @@ def node_geometry(s, alpha_lo, alpha_hi, u, ymin):
     return valid, lna, y, bnode, blna
 
 
-def distance_weights(y, prior, ymin, density=None):
+def distance_weights(y, prior, ymin, density=None, quadrature="reference"):
     """exmarg/search/pe.py:260-286: ln of the weights that integrate the distance prior against
     a likelihood ratio linear in ln y between the points y (ascending).  prior 'volume' is exact;
-    'madau-dickinson' uses the trapezoid rule on 401 points per interval over density (lny, p_lny)."""
+    'madau-dickinson' uses the trapezoid rule on 401 points per interval over density (lny, p_lny).
+    quadrature='gl64': both by 64-point Gauss-Legendre in ln y on every interval (numpy's leggauss)."""
     x = np.log(y)
     w = np.zeros_like(x)
+    gx, gw = np.polynomial.legendre.leggauss(64)
     for i in range(x.size - 1):
         a, b = x[i], x[i + 1]
         h = b - a
-        if prior == "volume":
+        if quadrature == "gl64":
+            t = 0.5 * (a + b) + 0.5 * h * gx
+            f = 3.0 * ymin ** 3 * np.exp(-3.0 * t) if prior == "volume" else \
+                np.interp(t, density[0], density[1], left=0.0, right=0.0)
+            w[i] += 0.5 * np.sum(gw * f * (b - t))
+            w[i + 1] += 0.5 * np.sum(gw * f * (t - a))
+        elif prior == "volume":
             c, k = 3.0 * ymin ** 3, 3.0
             ea, eb = np.exp(-k * a), np.exp(-k * b)
             I0 = (ea - eb) / k
@@ -234,7 +242,7 @@ def distance_weights(y, prior, ymin, density=None):
         return np.log(w)
 
 
-def ln_weights(yN, prior, ymin, density=None):
+def ln_weights(yN, prior, ymin, density=None, quadrature="reference"):
     """exmarg/search/pe.py:321-327: lnW (n_node + 1, n_template), -inf where a template has no point"""
     lnW = np.full(yN.shape, -np.inf)
     for m in range(yN.shape[1]):
@@ -242,7 +250,7 @@ def ln_weights(yN, prior, ymin, density=None):
         if pts.size < 2:
             raise ValueError("template %d reaches fewer than two store nodes" % m)
         order = pts[np.argsort(yN[pts, m])]
-        lnW[order, m] = distance_weights(yN[order, m], prior, ymin, density)
+        lnW[order, m] = distance_weights(yN[order, m], prior, ymin, density, quadrature)
     return lnW
 
 
@@ -296,8 +304,9 @@ def node_values(traj, store, geometry, groups, times):
 
 def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0.1267, nodes_per_launch=6,
                  n_loud=1024, n_random=1024, seed=0, precision="fp64", density=None, times=None,
-                 return_parts=False, bank_rows=None, n_bank=None):
+                 return_parts=False, bank_rows=None, n_bank=None, quadrature="reference"):
     """exmarg/search/pe.py:289-346 for the segments of seg (read_segments output).
+    quadrature='gl64': the distance prior by 64-point Gauss-Legendre (distance_weights).
 
     W (n_template, n_freq) complex template factors, u (n_template,) their powers.
     times: optional list (one per segment) of (sel, lw) to use instead of select_times
@@ -310,7 +319,7 @@ def pe_intrinsic(seg, W, u, M, q, chi, lo, n_time, store, prior="volume", ymin=0
     yN = geometry[2]
     nn = store.s.size
     groups = [list(range(g, min(g + nodes_per_launch, nn))) for g in range(0, nn, nodes_per_launch)]
-    lnW = ln_weights(yN, prior, ymin, density)
+    lnW = ln_weights(yN, prior, ymin, density, quadrature)
     nseg = seg["rows"].size
     out = np.full((nseg, u.size), -np.inf)
     parts = []

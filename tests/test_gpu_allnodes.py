@@ -1,0 +1,44 @@
+"""All 53 signal-power nodes of the production grid (s = 4.26e-3 ... 4000, the grid of data/tables/s_grid.npz)
+in one analysis, against the oracle at the reference's precision: every template walks every node it reaches,
+the boundary points included, for both gather kernels.  The tables keep the production node grid and lag
+count of an 8 s, 256 Hz analysis (43 lags) with 100 x 109 (beta, Delta) points, so the host oracle's store
+stays near 5 GB."""
+
+import numpy as np
+import pytest
+
+import exmarg_b200 as eb
+from exmarg_b200 import _lib, synth
+from oracle import restate
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    spec = synth.TableSpec(ntau=43, nb=100, nd=109)
+    s_nodes = synth.S_NODES_PROD
+    store = synth.MemoryStore(spec, s_nodes, 77, tables=restate.gen_tables(spec, s_nodes, 77))
+    seg = synth.make_segments(1, 6060, T=8.0, fmax=256.0, snr=18.0, mc=22.0, q=0.7, chi=0.1)
+    rows = synth.make_bank(2048, 11)[::43]                # 48 templates across the whole bank
+    bank = eb.MassBank(rows[:, 0], rows[:, 1], rows[:, 2], seg, "b200")
+    o = restate.pe_intrinsic(restate.read_segments(seg), bank.W, bank.u, bank.M, bank.q, bank.chi, bank.lo,
+                             bank.n_time, store, n_loud=1024, n_random=1024, seed=0, precision="ref")
+    return store, seg, bank, o
+
+
+@pytest.mark.parametrize("shape", ["20w x2", "runs 20w"])
+def test_all_53_nodes_match_reference_precision_oracle(case, shape):
+    store, seg, bank, o = case
+    ctx = eb.prepare(bank, store, "volume", 0.1267)
+    ctx.set_gather_cfg(_lib.GATHER_SHAPES.index(shape), 100)
+    try:
+        res = eb.pe_intrinsic(seg, bank, store, n_loud=1024, n_random=1024)
+    finally:
+        ctx.set_gather_cfg(0, 100)
+    valid = restate.node_geometry(store.s, store.alpha_lo, store.alpha_hi, bank.u, 0.1267)[0]
+    assert valid.any(axis=1).sum() >= 45 and valid.sum(axis=0).min() >= 40   # 43-47 nodes per template
+    assert np.abs(res["ln_b"] - o["ln_b"]).max() <= 1e-5
+    fin = np.isfinite(o["ln_lambda"])
+    assert fin.all() and np.array_equal(fin, np.isfinite(res["ln_lambda"]))
+    assert np.abs(res["ln_lambda"] - o["ln_lambda"]).max() <= 1e-4

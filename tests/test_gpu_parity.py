@@ -185,3 +185,19 @@ def test_errors_are_reported():
     # the context is still usable after the errors
     res = eb.pe_intrinsic(fx.seg, bank, fx.store, n_loud=fx.n_loud, n_random=fx.n_random)
     assert np.abs(res["ln_b"] - fx.ln_b).max() <= TOL_LNB
+
+
+@pytest.mark.parametrize("name", ["config1", "alltimes_md"])
+def test_gl64_quadrature_matches_oracle(name):
+    # the 64-point Gauss-Legendre distance quadrature on the device against the oracle's (numpy's rule)
+    fx = Fixture(name)
+    bank = fx.b200_bank()
+    res = eb.pe_intrinsic(fx.seg, bank, fx.store, prior=fx.prior_arg, ymin=fx.ymin, n_loud=fx.n_loud,
+                          n_random=fx.n_random, seed=0, quadrature="gl64")
+    seg = restate.read_segments(fx.seg)
+    M, q, chi = (fx.rows[:, i] for i in range(3))
+    o = restate.pe_intrinsic(seg, fx.W, fx.u, M, q, chi, fx.lo, fx.n_time, fx.store, prior=fx.prior, ymin=fx.ymin,
+                             n_loud=fx.n_loud, n_random=fx.n_random, seed=0, precision="ref", density=fx.density,
+                             quadrature="gl64")
+    assert np.abs(res["ln_b"] - o["ln_b"]).max() <= TOL_LNB
+    assert np.abs(res["ln_lambda"] - o["ln_lambda"]).max() <= TOL_LNL
