@@ -65,7 +65,7 @@ void exm_ensure(exm_ctx *ctx, dbuf &b, size_t bytes)
 
 static void free_slot(exm_ctx *ctx, exm_slot &s)
 {
-    dbuf *all[] = {&s.traj, &s.fft, &s.keys, &s.picks, &s.rej, &s.sel, &s.hist, &s.win, &s.cnt,
+    dbuf *all[] = {&s.traj, &s.trajlo, &s.fft, &s.keys, &s.picks, &s.rej, &s.sel, &s.hist, &s.win, &s.cnt,
                    &s.desc, &s.tside, &s.part, &s.lnl, &s.lnb, &s.dev_err, &s.din};
     for (dbuf *b : all) exm_free(ctx, *b);
     if (s.hostin.p) cudaFreeHost(s.hostin.p);
@@ -868,6 +868,7 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
 {
     const size_t nmc = rs.nmc_max, nt = ctx->nt, nf = ctx->nfreq;
     exm_ensure(ctx, sl.traj, 2 * nmc * nt * sizeof(float2));
+    exm_ensure(ctx, sl.trajlo, 2 * nmc * nt * sizeof(float));
     exm_ensure(ctx, sl.fft, 2 * nmc * nt * sizeof(double2));
     const size_t n_draws = rs.K > 0 ? (((size_t)ctx->nm * rs.S + EXM_MAX_REJ + 63) / 64) * 64 : 0;
     exm_ensure(ctx, sl.keys, std::max<size_t>(rs.K > 0 ? nmc * nt : 1, n_draws) * sizeof(uint32_t));
@@ -1243,6 +1244,7 @@ extern "C" int exm_set_trajectories(exm_ctx *ctx, const float *traj)
             for (size_t t = 0; t < nt; ++t) dst[t] = make_float2(lq[t], ph[t]);
         }
     EXM_CUDA(cudaMemcpy(sl.traj.p, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
+    EXM_CUDA(cudaMemset(sl.trajlo.p, 0, sizeof(float) * h.size()));   // float32 trajectories: no residual
     ctx->traj_ok = true;
     ctx->times_ok = false;
     ctx->cur_nwalk = ctx->nt;

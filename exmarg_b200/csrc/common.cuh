@@ -54,6 +54,7 @@ struct dbuf {
 // per-segment workspace of the analysis pipeline
 struct exm_slot {
     dbuf traj;      // float2 [2][nm][nt]: (ln|z|, arg z) of H then L
+    dbuf trajlo;    // float [2][nm][nt]: ln|z| - float(ln|z|) (0 for trajectories uploaded as float32)
     dbuf fft;       // double2 [2][nm][nt]: the padded rows and their transforms
     dbuf keys;      // uint32 [nm][nt]: selection scores as ordered integers
     dbuf picks;     // int32 [nm][S]: random ranks into the rest

@@ -81,8 +81,11 @@ struct TapGeom {
 // them per node, exmarg/search/gather.py:50-82): the plane pair p and the weight w
 // of plane p + 1, beta-hat = ln|z_L| 2/dbeta - ln(u)/dbeta as floor + fraction,
 // and the Delta coordinate of the unclamped-beta case as (d0, fd).
-__device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, double boff, const TapGeom &g, int &p, float &w,
-                                             int &ib, float &fb, int &d0, float &fd)
+// ln|z| enters as its float32 value plus the filter's float32 residual (llo, hlo: ln|z| - float(ln|z|), zero for
+// trajectories given as float32), so beta-hat and Delta see the filter's float64 value; the phases stay float32
+// and are subtracted in float32, as the reference does.
+__device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, float llo, float hlo, double boff, const TapGeom &g,
+                                             int &p, float &w, int &ib, float &fb, int &d0, float &fd)
 {
     double x3 = (double)(h.y - l.y) * g.rph;   // float32 difference, float64 scale, as the reference
     if (x3 < 0.0) x3 += EXM_NPHI;
@@ -98,11 +101,12 @@ __device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, double boff, co
         p = EXM_NPHI - 1 - c0;
         w = (float)(1.0 - fc);
     }
-    const double bh = (double)l.x * g.rdb + boff;
+    const double aL = (double)l.x + (double)llo, aH = (double)h.x + (double)hlo;
+    const double bh = aL * g.rdb + boff;
     const double fl = floor(bh);
     ib = (int)fmax(fmin(fl, 1023.0), -1024.0);
     fb = (float)(bh - fl);
-    double xd = ((double)h.x - (double)l.x) * g.rdd + g.offd;
+    double xd = (aH - aL) * g.rdd + g.offd;
     if (xd < 0.0) xd = 0.0; else if (xd > g.nd - 1 - 1e-6) xd = g.nd - 1 - 1e-6;
     d0 = (int)xd;
     fd = (float)(xd - d0);
@@ -112,7 +116,8 @@ __device__ __forceinline__ void exm_tap_geom(float2 l, float2 h, double boff, co
 // node table Tn (padded rows of ndp elements, value = scale * element), lag row r;
 // lw added by the caller
 template <typename TE>
-__device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, int r, const TE *__restrict__ Tn,
+__device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, float llo, float hlo, double offb, int r,
+                                               const TE *__restrict__ Tn,
                                                float scale, int nphif, int nb, int nd, int ndp, double rph, double rdb,
                                                double rdd, double offd)
 {
@@ -123,7 +128,7 @@ __device__ __forceinline__ double exm_tap_fp64(float2 l, float2 h, double offb, 
     c0 = c0 < 0 ? 0 : (c0 > EXM_NPHI - 1 ? EXM_NPHI - 1 : c0);
     const double fc = x3 - c0;
     const int c1 = (c0 + 1) % EXM_NPHI;
-    const double aH = h.x, aL = l.x;
+    const double aH = (double)h.x + (double)hlo, aL = (double)l.x + (double)llo;
     const double xbr = aL * rdb + offb;
     double xb = xbr;
     if (xb < 0.0) xb = 0.0; else if (xb > nb - 1 - 1e-6) xb = nb - 1 - 1e-6;

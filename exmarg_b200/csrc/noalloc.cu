@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(256) k_gather_noalloc(NoAllocArgs a)
             if (i1 >= nt) i1 -= nt;
             const float2 l = make_float2(a.lqL[mid * nt + t], a.phL[mid * nt + t]);
             const float2 h = make_float2(a.lqH[mid * nt + i1], a.phH[mid * nt + i1]);
-            double acc = exm_tap_fp64<TE>(l, h, offb, r, (const TE *)a.T + tb * a.tstride, a.tsc[tb], a.nphif, a.nb,
+            double acc = exm_tap_fp64<TE>(l, h, 0.f, 0.f, offb, r, (const TE *)a.T + tb * a.tstride, a.tsc[tb], a.nphif, a.nb,
                                           a.nd, a.ndp, a.rph, a.rdb, a.rdd, a.offd);
             if (a.sel) acc += (double)a.lw[mid * a.nwalk + k];
             if (acc > m) {

@@ -96,7 +96,7 @@ static size_t workspace_estimate(const exm_server *s, const SrvBank &b)
     const size_t nwalk = s->n_loud > 0 ? (size_t)(s->n_loud + s->n_random) : nt;
     const size_t per_lag = nmc * nwalk * 20;
     const size_t rc = std::max<size_t>(1, std::min<size_t>((size_t)p->ntau, ((size_t)8 << 30) / std::max<size_t>(per_lag, 1)));
-    size_t by = 2 * nmc * nt * (16 + 8);
+    size_t by = 2 * nmc * nt * (16 + 8 + 4);   // FFT rows, trajectories, ln|z| residuals
     by += std::max(nmc * nt, nm * 1024 + 4096) * 4 + nm * 1024 * 4;
     by += nmc * nwalk * 4 + rc * 48 * (nmc + 1) * 4 + rc * per_lag;
     by += (size_t)(p->nn + 1) * p->ntau * nm * 8 + nm * 8 * 12 + nm * (size_t)b.nfreq * 8;

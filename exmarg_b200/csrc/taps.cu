@@ -20,6 +20,7 @@
 
 struct TapArgs {
     const float2 *H, *L;
+    const float *Hlo, *Llo;   // residuals of ln|z| (filter output) or zeros
     const int32_t *sel;
     const double *boff;   // [nmc] -ln(u)/dbeta of the chunk's templates
     const int *tau;       // [ntau]
@@ -54,11 +55,12 @@ __device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t,
 struct WalkCache {
     int *t;
     float2 *l;
+    float *llo;
     int *flag;
     bool on;
 };
 
-__device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 *L, WalkCache &wc)
+__device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 *L, const float *Llo, WalkCache &wc)
 {
     if (!wc.on) return;
     for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
@@ -67,20 +69,23 @@ __device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 
         wc.t[k] = t;
         wc.flag[k] = flag;
         wc.l[k] = L[t];
+        wc.llo[k] = Llo[t];
     }
     __syncthreads();
 }
 
-__device__ __forceinline__ void walk_at(const TapArgs &a, int i, const float2 *L, const WalkCache &wc, int k, int &t,
-                                        int &flag, float2 &l)
+__device__ __forceinline__ void walk_at(const TapArgs &a, int i, const float2 *L, const float *Llo, const WalkCache &wc,
+                                        int k, int &t, int &flag, float2 &l, float &llo)
 {
     if (wc.on) {
         t = wc.t[k];
         flag = wc.flag[k];
         l = wc.l[k];
+        llo = wc.llo[k];
     } else {
         tap_time(a, i, k, t, flag);
         l = L[t];
+        llo = Llo[t];
     }
 }
 
@@ -99,13 +104,15 @@ __global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
         for (int q = threadIdx.x; q < EXM_HB_N; q += blockDim.x) hb[q] = 0;
     const int nt = a.g.nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
+    const float *Hlo = a.Hlo + (long long)i * nt, *Llo = a.Llo + (long long)i * nt;
     const double boff = a.boff[i];
     WalkCache wc;
     wc.on = a.nwalk <= TAP_CACHE;
     wc.l = (float2 *)wsm;
     wc.t = (int *)(wc.l + TAP_CACHE);
     wc.flag = wc.t + TAP_CACHE;
-    load_walk(a, i, L, wc);
+    wc.llo = (float *)(wc.flag + TAP_CACHE);
+    load_walk(a, i, L, Llo, wc);
     for (int rl = 0; rl < rc; ++rl) {
         for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) c[q] = 0;
         __syncthreads();
@@ -113,12 +120,13 @@ __global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
         for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
             int t, flag;
             float2 l;
-            walk_at(a, i, L, wc, k, t, flag, l);
+            float llo;
+            walk_at(a, i, L, Llo, wc, k, t, flag, l, llo);
             int i1 = t + tau0;
             if (i1 >= nt) i1 -= nt;
             int p, ib, d0;
             float w, fb, fd;
-            exm_tap_geom(l, H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+            exm_tap_geom(l, H[i1], llo, Hlo[i1], boff, a.g, p, w, ib, fb, d0, fd);
             // warp-aggregated increments: one atomic per distinct bin in the warp
             const unsigned pm = __match_any_sync(__activemask(), p);
             if ((threadIdx.x & 31) == __ffs(pm) - 1) atomicAdd(&c[p], __popc(pm));
@@ -192,13 +200,15 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nt = a.g.nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
+    const float *Hlo = a.Hlo + (long long)i * nt, *Llo = a.Llo + (long long)i * nt;
     const double boff = a.boff[i];
     WalkCache wc;
     wc.on = a.nwalk <= TAP_CACHE;
     wc.l = (float2 *)wsm;
     wc.t = (int *)(wc.l + TAP_CACHE);
     wc.flag = wc.t + TAP_CACHE;
-    load_walk(a, i, L, wc);
+    wc.llo = (float *)(wc.flag + TAP_CACHE);
+    load_walk(a, i, L, Llo, wc);
     const unsigned lt = (1u << lane) - 1u;
     const int C0 = a.win[0], Rh = a.win[1 + EXM_MAX_NODES];
     for (int rl = 0; rl < rc; ++rl) {
@@ -216,10 +226,11 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
             float w = 0.f, fb = 0.f, fd = 0.f;
             if (k < a.nwalk) {
                 float2 l;
-                walk_at(a, i, L, wc, k, t, flag, l);
+                float llo;
+                walk_at(a, i, L, Llo, wc, k, t, flag, l, llo);
                 int i1 = t + tau0;
                 if (i1 >= nt) i1 -= nt;
-                exm_tap_geom(l, H[i1], boff, a.g, p, w, ib, fb, d0, fd);
+                exm_tap_geom(l, H[i1], llo, Hlo[i1], boff, a.g, p, w, ib, fb, d0, fd);
             }
             const unsigned peers = __match_any_sync(0xffffffffu, p);
             const int rk = __popc(peers & lt);
@@ -324,6 +335,8 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     TapArgs a;
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ci.nmc * nt;
+    a.Hlo = (const float *)sl.trajlo.p;
+    a.Llo = a.Hlo + (size_t)ci.nmc * nt;
     a.sel = (const int32_t *)sl.sel.p;
     a.boff = (const double *)ctx->d_bhat_off.p + ci.m_base;
     a.tau = (const int *)ctx->d_tau.p;
@@ -347,7 +360,7 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     a.pitch = exm_desc_pitch(a.per_lag);
     if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
     EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
-    const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int)) : 0;
+    const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int) + sizeof(float)) : 0;
     exm_allow_smem(ctx, (const void *)k_tap_count, wsm);
     exm_allow_smem(ctx, (const void *)k_tap_scatter, wsm);
     a.win = (const int *)sl.win.p;

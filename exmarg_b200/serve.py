@@ -34,7 +34,7 @@ def workspace_bytes(nm, n_time, n_nodes, n_lags, nfreq, nwalk):
     nmc = min(nm, 8192)
     per_lag = nmc * nwalk * 20
     rc = max(1, min(n_lags, (8 << 30) // max(per_lag, 1)))
-    b = 2 * nmc * n_time * (16 + 8)                      # FFT buffer + trajectories
+    b = 2 * nmc * n_time * (16 + 8 + 4)                  # FFT buffer + trajectories + ln|z| residuals
     b += max(nmc * n_time, nm * 1024 + 4096) * 4 + nm * 1024 * 4
     b += nmc * nwalk * 4 + rc * 48 * (nmc + 1) * 4 + rc * per_lag
     b += (n_nodes + 1) * n_lags * nm * 8 + nm * 8 * 12 + nm * nfreq * 8
