@@ -17,10 +17,9 @@ EXM_OK, EXM_ERR_ARG, EXM_ERR_OOM, EXM_ERR_CUDA, EXM_ERR_TIMEOUT, EXM_ERR_STATE =
 DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 QUAD_GL64 = 16   # OR'ed into the prior: 64-point Gauss-Legendre distance quadrature
-# the plane gather's launch shapes, in exm_autotune / exm_set_gather_cfg order: k_gather_planes (warps per
-# block x taps per register group), then k_gather_runs (warps per block)
-GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2",
-                 "runs 16w", "runs 20w", "runs 24w")
+# the plane gather's launch shapes, in exm_autotune / exm_set_gather_cfg order (warps per block x taps
+# per register group)
+GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2")
 
 # every symbol include/exmarg_b200.h declares
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",

@@ -1122,8 +1122,6 @@ extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, in
     const bool tim = ctx->tim_on;
     ctx->tim_on = false;
     auto time_gather = [&]() {
-        if (exm_gather_cfg_sorted(ctx->gather_cfg) != sl.desc_sorted)   // the shape reads the other order
-            exm_run_taps(ctx, sl, ci, 0, ctx->ntau, true);
         exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);   // warm-up (and function attributes)
         EXM_CUDA(cudaEventRecord(e0, ctx->stream));
         for (int r = 0; r < std::max(1, reps); ++r) exm_run_gather_planes(ctx, sl, ci, 0, ctx->ntau);
@@ -1162,7 +1160,6 @@ extern "C" int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, in
     ctx->gather_chunk_pct = best_pct;
     ctx->tim_on = tim;
     ctx->gather_cfg = arg;
-    if (exm_gather_cfg_sorted(arg) != sl.desc_sorted) exm_run_taps(ctx, sl, ci, 0, ctx->ntau, true);
     if (best_cfg) *best_cfg = arg;
     if (best_chunk_pct) *best_chunk_pct = best_pct;
     cudaEventDestroy(e0);

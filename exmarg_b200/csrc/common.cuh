@@ -72,7 +72,6 @@ struct exm_slot {
     dbuf hostin;    // pinned host staging (d_H, d_L)
     dbuf din;       // device copy of d_H, d_L complex128 and sig2
     int nwalk = 0, rc = 0;
-    bool desc_sorted = false;   // descriptors as the scatter wrote them (k_gather_runs), not lane-interleaved
 };
 
 #define EXM_MAX_REJ 4096

@@ -716,462 +716,11 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     }
 }
 
-// ------------------------------------------------------------------ the run-group gather (k_gather_runs)
-//
-// Same block decomposition, staging ring, exact-path queue and accumulator sets as k_gather_planes; the
-// consumers walk a plane pair differently.  A warp is four groups of EXM_RG lanes, and a group takes whole
-// (template, pair) runs: its lanes step through one template's taps EXM_RG * EXM_RU at a time (lane l of the
-// group takes taps s + u * EXM_RG + l), each lane keeps one running log-sum-exp, and when the run ends the
-// group combines its lanes with three shuffles and its first lane merges the run into the template's
-// accumulator.  There is no per-tap template bookkeeping and no merge across lanes of different templates.
-// The templates of a pair are split among the groups by tap count (a template goes to the group in whose
-// share its run starts), from the pair's run offsets that the producer warp copies to shared memory one pair
-// ahead; the split is fixed, so every run is reduced in the same order and results are reproducible.
-// Descriptors are read in sorted order (no lane interleave): a group's loads of one step are contiguous.
-#define EXM_RG 8    // lanes of a run group
-#define EXM_RU 2    // taps per lane and step
-
-struct RunsCtx {
-    const uint4 *descr;
-    const int32_t *tsr;
-    unsigned s0, s1;            // staged windows of planes p, p + 1
-    float sc;
-    int m_base, lo, n, k, r, sh, up, edge;
-    float ckf, lw;
-    unsigned q, qn;             // this warp's exact-path queue for the pair and its count
-};
-
-// one step of a group: the EXM_RU taps of this lane at positions pos + u * EXM_RG (already loaded in d),
-// valid below end; merged into the lane's running (cB, cE, cS)
-template <bool BND, typename TE>
-__device__ __forceinline__ void runs_step(const PlaneArgs &a, const RunsCtx &c, const uint4 *d, int pos, int end,
-                                          int il, float bfr, int bsh, float &cB, float &cE, float &cS,
-                                          unsigned &n_slow)
-{
-    constexpr int WD = TabElem<TE>::wd;
-    const int gl = threadIdx.x & (EXM_RG - 1);
-    int o[EXM_RU];
-    bool fast[EXM_RU], valid[EXM_RU];
-    float fbf[EXM_RU], fd[EXM_RU], w[EXM_RU], lwv[EXM_RU], vB[EXM_RU], vE[EXM_RU];
-#pragma unroll
-    for (int u = 0; u < EXM_RU; ++u) {
-        valid[u] = pos + u * EXM_RG + gl < end;
-        const float sfr = __uint_as_float(d[u].x) + bfr;
-        fd[u] = __uint_as_float(d[u].y);
-        w[u] = __uint_as_float(d[u].z & 0x7FFFFFFFu);
-        lwv[u] = (d[u].z >> 31) ? c.lw : 0.f;
-        const int rd = (int)((d[u].w >> 11) & 0xFFu);
-        const int rb0 = ((int)(d[u].w << 21)) >> 21;
-        const int cy = sfr >= 1.f;
-        fbf[u] = cy ? sfr - 1.f : sfr;
-        const int rb = rb0 + cy + bsh;
-        fast[u] = (unsigned)rb <= (unsigned)c.up && rd <= WD - 2 && !(rb == c.edge && fbf[u] > 0.999999f);
-        o[u] = fast[u] ? rb * WD + rd : 0;
-    }
-#pragma unroll
-    for (int u = 0; u < EXM_RU; ++u) {
-        interp_window<TE>((const TE *)(exm_gsm + c.s0), (const TE *)(exm_gsm + c.s1), o[u], fbf[u], fd[u], w[u], c.sc,
-                          vB[u], vE[u]);
-        if (!valid[u]) {   // no tap here: a value below every tap, so the running maximum stays
-            vB[u] = -1e30f;
-            vE[u] = 0.f;
-        }
-    }
-#pragma unroll
-    for (int u = 0; u < EXM_RU; ++u) {
-        const bool sl = valid[u] && !fast[u];
-        float wt = valid[u] ? 1.f : 0.f;
-        if (__any_sync(0xffffffffu, sl)) {
-            const int lane = threadIdx.x & 31;
-            const unsigned m = __ballot_sync(0xffffffffu, sl);
-            int *qn = (int *)(exm_gsm + c.qn);
-            const int n0 = *qn;
-            const int qp = n0 + __popc(m & ((1u << lane) - 1u));
-            __syncwarp();
-            if (sl) {
-                ++n_slow;
-                const int j = pos + u * EXM_RG + gl;
-                if (qp < EXM_SLOWQ) {   // the producer adds it; this lane skips it
-                    ((int2 *)(exm_gsm + c.q))[qp] =
-                        make_int2(j, il | (BND ? 1 << 30 : 0) | (int)((d[u].z >> 31) << 29));
-                    vB[u] = -1e30f;
-                    vE[u] = 0.f;
-                    lwv[u] = 0.f;
-                    wt = 0.f;
-                } else {
-                    const double v = slow_tap<BND, TE>(a, il, c.tsr[j], c.k, c.r, c.m_base, c.sc);
-                    split_double(v, vB[u], vE[u]);
-                }
-            }
-            if (lane == 0) *qn = min(EXM_SLOWQ, n0 + __popc(m));
-            __syncwarp();
-        }
-        lse_merge(cB, cE, cS, vB[u], vE[u] + lwv[u], wt);
-    }
-}
-
-// the first template at or after j (below j1) with a non-empty run (and, for the boundary pass, whose
-// boundary point lies at this node)
-template <bool BND>
-__device__ __forceinline__ int runs_next(const int *offs, const int *bnode, int lo, int k, int j, int j1)
-{
-    while (j < j1 && (offs[j + 1] == offs[j] || (BND && bnode[lo + j] != k))) ++j;
-    return j;
-}
-
-// one pass over templates [t0, t1) of pair p: group g of the warp takes templates [gb[g], gb[g + 1])
-template <bool BND, typename TE>
-__device__ __forceinline__ void runs_pass(const PlaneArgs &a, const RunsCtx &c, const int *offs, const int *gb,
-                                          const int *bnode, const float *bcf, const int *bsh_t, float *accB,
-                                          float *accE, float *accS, unsigned &n_slow)
-{
-    const int lane = threadIdx.x & 31, gl = lane & (EXM_RG - 1);
-    const int gid = (threadIdx.x >> 5) * (32 / EXM_RG) + (lane / EXM_RG);
-    const int j1 = gb[gid + 1];
-    int j = runs_next<BND>(offs, bnode, c.lo, c.k, gb[gid], j1);
-    const int gend = offs[j1];                  // no load at or beyond the group's last run
-    bool active = j < j1;
-    int pos = active ? offs[j] : gend, end = active ? offs[j + 1] : gend;
-    float bfr = active ? (BND ? bcf[j] : c.ckf) : 0.f;
-    int bsh = active ? (BND ? bsh_t[j] : c.sh) : 0;
-    uint4 d[EXM_RU];
-#pragma unroll
-    for (int u = 0; u < EXM_RU; ++u) {
-        const int x = pos + u * EXM_RG + gl;
-        d[u] = x < gend ? __ldg(c.descr + x) : make_uint4(0u, 0u, 0u, 0u);
-    }
-    float cB = -1e30f, cE = 0.f, cS = 0.f;
-    while (__any_sync(0xffffffffu, active)) {
-        // the next step's descriptors: this run's, or the run that follows it in memory
-        const int npos = (pos + EXM_RG * EXM_RU < end) ? pos + EXM_RG * EXM_RU : end;
-        uint4 nd[EXM_RU];
-#pragma unroll
-        for (int u = 0; u < EXM_RU; ++u) {
-            const int x = npos + u * EXM_RG + gl;
-            nd[u] = x < gend ? __ldg(c.descr + x) : make_uint4(0u, 0u, 0u, 0u);
-        }
-        // one call for every lane (its votes are warp-wide): an idle group's taps are all invalid
-        runs_step<BND, TE>(a, c, d, active ? pos : 0, active ? end : 0, active ? j + c.lo - c.m_base : 0,
-                           active ? bfr : 0.f, active ? bsh : 0, cB, cE, cS, n_slow);
-        const bool fin = active && npos == end;
-        int npos2 = npos;
-        if (__any_sync(0xffffffffu, fin)) {
-            // a finishing group's lanes hold partials of one template: combine them in copies (the lanes of
-            // groups still inside a run keep their own partials), the first lane merges the total
-            float tB = cB, tE = cE, tS = cS;
-#pragma unroll
-            for (int o = EXM_RG / 2; o > 0; o >>= 1) {
-                const float B2 = __shfl_xor_sync(0xffffffffu, tB, o);
-                const float E2 = __shfl_xor_sync(0xffffffffu, tE, o);
-                const float S2 = __shfl_xor_sync(0xffffffffu, tS, o);
-                lse_merge(tB, tE, tS, B2, E2, S2);
-            }
-            if (fin) {
-                if (gl == 0 && tS > 0.f) {
-                    float b = accB[j], x = accE[j], s = accS[j];
-                    lse_merge(b, x, s, tB, tE, tS);
-                    accB[j] = b;
-                    accE[j] = x;
-                    accS[j] = s;
-                }
-                cB = -1e30f;
-                cE = 0.f;
-                cS = 0.f;
-                j = runs_next<BND>(offs, bnode, c.lo, c.k, j + 1, j1);
-                active = j < j1;
-                if (active) {
-                    npos2 = offs[j];
-                    end = offs[j + 1];
-                    bfr = BND ? bcf[j] : c.ckf;
-                    bsh = BND ? bsh_t[j] : c.sh;
-                }
-            }
-        }
-        if (active && npos2 != npos) {   // the next run does not follow in memory (boundary pass): load it
-#pragma unroll
-            for (int u = 0; u < EXM_RU; ++u) {
-                const int x = npos2 + u * EXM_RG + gl;
-                nd[u] = x < gend ? __ldg(c.descr + x) : make_uint4(0u, 0u, 0u, 0u);
-            }
-        }
-        pos = npos2;
-#pragma unroll
-        for (int u = 0; u < EXM_RU; ++u) d[u] = nd[u];
-    }
-}
-
-// split templates [t0, t1) of a pair among ng groups by tap count: gb[g] = the first template whose run
-// starts at or after t0's offset + g * taps / ng (one lane per bound, binary search in shared memory)
-__device__ __forceinline__ void runs_bounds(const int *offs, int t0, int t1, int ng, int *gb)
-{
-    const int lane = threadIdx.x & 31;
-    const long long base = offs[t0], tot = offs[t1] - offs[t0];
-    for (int g = lane; g <= ng; g += 32) {
-        int x;
-        if (g == 0) x = t0;
-        else if (g == ng) x = t1;
-        else {
-            const long long tgt = base + tot * g / ng;
-            int lo2 = t0, hi2 = t1;
-            while (lo2 < hi2) {
-                const int mid = (lo2 + hi2) >> 1;
-                if (offs[mid] < tgt) lo2 = mid + 1; else hi2 = mid;
-            }
-            x = lo2;
-        }
-        gb[g] = x;
-    }
-}
-
-template <int NW, typename TE>
-__global__ void __launch_bounds__(NW * 32, 1) k_gather_runs(const __grid_constant__ CUtensorMap tmap,
-                                                              const __grid_constant__ PlaneArgs a)
-{
-    constexpr int NC = NW - 1;                  // consumer warps
-    constexpr int NG = NC * (32 / EXM_RG);      // run groups
-    constexpr int SLOT = slot_elems<TE>();
-    constexpr unsigned SLOT_B = slot_bytes<TE>();
-    unsigned char *smem = exm_gsm;
-    TE *win = (TE *)smem;
-    uint64_t *full = (uint64_t *)(smem + 3 * SLOT_B);   // [3] plane staged in slot s
-    uint64_t *done = full + 3;                          // [2] every consumer is done with a pair (parity)
-    const int tch = a.tch;
-    // accumulator sets (B, E, S) of tch floats each: regular pairs of parity 0 / 1, the producer's exact
-    // taps; the same three for boundary points; then bcf, bsh; then per pair parity the run offsets of the
-    // block's templates (tch + 1) and the group bounds of the regular and the boundary pass (NG + 1 each)
-    const unsigned acc_o = 3 * SLOT_B + 64;
-    float *acc = gsm_f(acc_o);
-    float *bcf = acc + 18 * tch;
-    int *bsh = (int *)(bcf + tch);
-    int *offs_all = bsh + tch;                          // [2][tch + 1]
-    int *gb_all = offs_all + 2 * (tch + 1);             // [2][2][NG + 1]
-    const unsigned qcnt_o = (acc_o + 4u * (20u * tch + 2u * (tch + 1) + 4u * (NG + 1)) + 15u) & ~15u;
-    const unsigned qent_o = qcnt_o + 4u * 3 * 32;
-    int *qcnt = (int *)(smem + qcnt_o);
-    const int2 *qent = (const int2 *)(smem + qent_o);
-    __shared__ int bl_sh[2];
-    __shared__ unsigned bad_sh;
-
-    const int c_idx = blockIdx.x % a.nch;
-    const int k = (blockIdx.x / a.nch) % a.nn;
-    const int rl = blockIdx.x / (a.nch * a.nn), r = a.r0 + rl;
-    const int lo0 = max(a.mlo[k], a.m_base), hi0 = min(a.mhi[k], a.m_base + a.nmc);
-    const int lo = lo0 + c_idx * tch;
-    const int hi = min(hi0, lo + tch);
-    if (lo >= hi) return;
-    const int n = hi - lo;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    if (tid == 0) {
-        bl_sh[0] = n;
-        bl_sh[1] = 0;
-        bad_sh = 0;
-    }
-    __syncthreads();
-    const int C0 = a.win[0], R0 = a.win[1 + k], Rh = a.win[1 + EXM_MAX_NODES];
-    const int sh = Rh + a.cki[k] - R0;
-    for (int j = tid; j < n; j += NW * 32) {
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            acc[(3 * q) * tch + j] = -1e30f;
-            acc[(3 * q + 1) * tch + j] = 0.f;
-            acc[(3 * q + 2) * tch + j] = 0.f;
-        }
-        if (a.bnode[lo + j] == k) {
-            const double cbv = a.cb[lo + j];
-            const double f = floor(cbv);
-            bsh[j] = (int)f - a.cki[k] + sh;
-            bcf[j] = (float)(cbv - f);
-            atomicMin(&bl_sh[0], j);
-            atomicMax(&bl_sh[1], j + 1);
-        }
-    }
-    const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1) + (lo - a.m_base);
-    // run offsets of pairs 0 and 1 (the producer copies pair p + 2's after pair p)
-    for (int i = tid; i < 2 * (n + 1); i += NW * 32) {
-        const int pp = i / (n + 1), j = i - pp * (n + 1);
-        offs_all[pp * (tch + 1) + j] = offr[pp * (a.nmc + 1) + j];
-    }
-    if (tid == 0) {
-        for (int s = 0; s < 3; ++s) mbar_init(&full[s], 1);
-        for (int s = 0; s < 2; ++s) mbar_init(&done[s], NC * 32);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    const int blo = bl_sh[0], bhi = bl_sh[1];
-    if (warp == NC)
-        for (int pp = 0; pp < 2; ++pp) {
-            runs_bounds(offs_all + pp * (tch + 1), 0, n, NG, gb_all + (pp * 2) * (NG + 1));
-            if (blo < bhi) runs_bounds(offs_all + pp * (tch + 1), blo, bhi, NG, gb_all + (pp * 2 + 1) * (NG + 1));
-        }
-    __syncthreads();
-    unsigned n_slow = 0, n_bnd = 0;
-
-    if (warp == NC) {
-        // ---------------------------------------------------------------- producer
-        const int32_t *tsr_all = a.tside + (long long)rl * a.per_lag;
-        int issued = 0;
-        if (a.stage) {
-            if (lane == 0)
-                for (int q = 0; q < 3 && q < a.nphif; ++q)
-                    tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
-            issued = min(3, a.nphif);
-        }
-        bool ok = true;
-        for (int p = 0; p < EXM_NPAIR; ++p) {
-            ok = ok && __all_sync(0xffffffffu, mbar_wait(&done[p & 1], (p >> 1) & 1, a.err, a.wait_cycles));
-            if (!ok) break;
-            // pair p is done everywhere: its offsets and bounds make way for pair p + 2's, published before
-            // plane p + 3 (which the consumers wait for before pair p + 2)
-            if (p + 2 < EXM_NPAIR) {
-                int *offs = offs_all + (p & 1) * (tch + 1);
-                const int *src = offr + (p + 2) * (a.nmc + 1);
-                for (int j = lane; j <= n; j += 32) offs[j] = src[j];
-                __syncwarp();
-                runs_bounds(offs, 0, n, NG, gb_all + ((p & 1) * 2) * (NG + 1));
-                if (blo < bhi) runs_bounds(offs, blo, bhi, NG, gb_all + ((p & 1) * 2 + 1) * (NG + 1));
-                __syncwarp();
-            }
-            if (a.stage && p + 3 < a.nphif) {
-                if (lane == 0) tma_load_plane(&tmap, &full[p % 3], win + (p % 3) * SLOT, C0, R0, p + 3, r, k, SLOT_B);
-                ++issued;
-            } else if (p + 2 < EXM_NPAIR) {
-                // no plane to stage (or staging off): publish the offsets with a plain release instead
-                __threadfence_block();
-            }
-            // the exact-path taps the consumers queued for pair p (as k_gather_planes)
-            {
-                const int par = p % 3;
-                const int cw = lane < NC ? qcnt[par * 32 + lane] : 0;
-                int incl = cw;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                const int excl = incl - cw;
-                for (int b0 = 0; b0 < total; b0 += 32) {
-                    const int i = b0 + lane;
-                    double v = 0.0;
-                    int tr = 0, bnd = 0;
-                    int wi = 0;
-                    for (int l = 1; l < NC; ++l) {
-                        const int el = __shfl_sync(0xffffffffu, excl, l);
-                        wi += (i < total && el <= i) ? 1 : 0;
-                    }
-                    const int wexcl = __shfl_sync(0xffffffffu, excl, wi);
-                    if (i < total) {
-                        const int2 e = qent[(par * 32 + wi) * EXM_SLOWQ + (i - wexcl)];
-                        const int il = e.y & 0x1FFF;
-                        bnd = (e.y >> 30) & 1;
-                        const int tm = tsr_all[e.x];
-                        v = bnd ? slow_tap<true, TE>(a, il, tm, k, r, a.m_base, a.tsc[k])
-                                : slow_tap<false, TE>(a, il, tm, k, r, a.m_base, a.tsc[k]);
-                        v += ((e.y >> 29) & 1) ? (double)a.lw : 0.0;
-                        tr = il + a.m_base - lo;
-                    }
-                    const int nb2 = min(32, total - b0);
-                    for (int qq = 0; qq < nb2; ++qq) {
-                        const double vq = __shfl_sync(0xffffffffu, v, qq);
-                        const int tq = __shfl_sync(0xffffffffu, tr, qq), bq = __shfl_sync(0xffffffffu, bnd, qq);
-                        if (lane == 0 && tq >= 0 && tq < n) {
-                            float B, E;
-                            split_double(vq, B, E);
-                            float *F = acc + (bq ? 15 : 6) * tch;
-                            float b = F[tq], x = F[tch + tq], sv = F[2 * tch + tq];
-                            lse_merge(b, x, sv, B, E, 1.f);
-                            F[tq] = b;
-                            F[tch + tq] = x;
-                            F[2 * tch + tq] = sv;
-                        }
-                    }
-                }
-                __syncwarp();
-            }
-        }
-        if (!ok) {
-            if (lane == 0) {
-                atomicOr(&bad_sh, 1u);
-                for (int q = max(0, issued - 3); q < issued; ++q) mbar_wait(&full[q % 3], (q / 3) & 1, a.err);
-            }
-        }
-    } else {
-        // ---------------------------------------------------------------- consumers
-        RunsCtx rc;
-        rc.descr = a.desc + (long long)rl * a.per_lag;
-        rc.tsr = a.tside + (long long)rl * a.per_lag;
-        rc.m_base = a.m_base;
-        rc.lo = lo;
-        rc.n = n;
-        rc.k = k;
-        rc.r = r;
-        rc.sh = sh;
-        rc.up = min(EXM_WB - 2, a.nb - 2 - R0);
-        rc.edge = a.nb - 2 - R0;
-        rc.ckf = a.ckf[k];
-        rc.sc = a.tsc[k];
-        rc.lw = a.lw;
-        bool ok = true;
-        for (int p = 0; p < EXM_NPAIR; ++p) {
-            ok = ok && __all_sync(0xffffffffu, mbar_wait(&full[p % 3], (p / 3) & 1, a.err, a.wait_cycles));
-            ok = ok && __all_sync(0xffffffffu,
-                                  mbar_wait(&full[(p + 1) % 3], ((p + 1) / 3) & 1, a.err, a.wait_cycles));
-            if (lane == 0) qcnt[(p % 3) * 32 + warp] = 0;
-            __syncwarp();
-            rc.qn = qcnt_o + 4u * ((p % 3) * 32 + warp);
-            rc.q = qent_o + 8u * (((p % 3) * 32 + warp) * EXM_SLOWQ);
-            if (ok) {
-                rc.s0 = (p % 3) * SLOT_B;
-                rc.s1 = ((p + 1) % 3) * SLOT_B;
-                const int *offs = offs_all + (p & 1) * (tch + 1);
-                float *set = acc + 3 * (p & 1) * tch;
-                runs_pass<false, TE>(a, rc, offs, gb_all + ((p & 1) * 2) * (NG + 1), a.bnode, bcf, bsh, set,
-                                     set + tch, set + 2 * tch, n_slow);
-                if (blo < bhi) {
-                    float *bset = acc + (9 + 3 * (p & 1)) * tch;
-                    n_bnd += (lane == 0 && warp == 0) ? (unsigned)(offs[bhi] - offs[blo]) : 0u;
-                    runs_pass<true, TE>(a, rc, offs, gb_all + ((p & 1) * 2 + 1) * (NG + 1), a.bnode, bcf, bsh,
-                                        bset, bset + tch, bset + 2 * tch, n_slow);
-                }
-            }
-            __syncwarp();
-            mbar_arrive(&done[p & 1]);
-        }
-        if (!ok && lane == 0) atomicOr(&bad_sh, 1u);
-    }
-    if (a.stats) {
-        const unsigned sl_ = __reduce_add_sync(0xffffffffu, n_slow), bd_ = __reduce_add_sync(0xffffffffu, n_bnd);
-        if (lane == 0 && (sl_ | bd_)) {
-            atomicAdd(&a.stats[0], (unsigned long long)sl_);
-            atomicAdd(&a.stats[1], (unsigned long long)bd_);
-        }
-    }
-    __syncthreads();
-    const bool ok = bad_sh == 0;
-    for (int j = tid; j < n; j += NW * 32) {
-        float B = acc[j], E = acc[tch + j], S = acc[2 * tch + j];
-        lse_merge(B, E, S, acc[3 * tch + j], acc[4 * tch + j], acc[5 * tch + j]);
-        lse_merge(B, E, S, acc[6 * tch + j], acc[7 * tch + j], acc[8 * tch + j]);
-        const double v = (ok && S > 0.f) ? (double)B + (double)E + log((double)S) : -INFINITY;
-        a.part[((long long)k * a.ntau + r) * a.nm_total + lo + j] = v;
-        if (j >= blo && j < bhi && a.bnode[lo + j] == k) {
-            float B2 = acc[9 * tch + j], E2 = acc[10 * tch + j], S2 = acc[11 * tch + j];
-            lse_merge(B2, E2, S2, acc[12 * tch + j], acc[13 * tch + j], acc[14 * tch + j]);
-            lse_merge(B2, E2, S2, acc[15 * tch + j], acc[16 * tch + j], acc[17 * tch + j]);
-            const double v2 = (ok && S2 > 0.f) ? (double)B2 + (double)E2 + log((double)S2) : -INFINITY;
-            a.part[((long long)a.nn * a.ntau + r) * a.nm_total + lo + j] = v2;
-        }
-    }
-}
-
-// launch shapes the autotuner chooses from: k_gather_planes (warps per block, taps per register group) and
-// k_gather_runs (warps per block; grp 0); warps include the producer
+// launch shapes the autotuner chooses from: (warps per block, taps per register group)
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{20, 2}, {16, 2}, {24, 2}, {24, 1}, {32, 1}, {32, 2},
-                                        {16, 0}, {20, 0}, {24, 0}};
+static const GatherCfg kGatherCfgs[] = {{20, 2}, {16, 2}, {24, 2}, {24, 1}, {32, 1}, {32, 2}};   // warps incl. producer
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -1182,22 +731,9 @@ static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t sm
     k_gather_planes<NW, GRP, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
 }
 
-template <int NW, typename TE>
-static void launch_runs(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
-{
-    exm_allow_smem(ctx, (const void *)k_gather_runs<NW, TE>, smem);
-    k_gather_runs<NW, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
-}
-
 template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
-    switch (cfg) {
-    case 6: launch_runs<16, TE>(ctx, a, grid, smem); return;
-    case 7: launch_runs<20, TE>(ctx, a, grid, smem); return;
-    case 8: launch_runs<24, TE>(ctx, a, grid, smem); return;
-    default: break;
-    }
     switch (cfg) {
     case 0: launch_planes<20, 2, TE>(ctx, a, grid, smem); break;
     case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
@@ -1220,38 +756,20 @@ static void launch_cfg(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, siz
 
 int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 
-// the gather of launch shape cfg reads its descriptors in sorted order (k_gather_runs), not lane-interleaved
-bool exm_gather_cfg_sorted(int cfg) { return cfg >= 0 && cfg < kNumGatherCfgs && kGatherCfgs[cfg].grp == 0; }
-
-// shared memory of a block with tch templates: the staging ring, barriers, and per template 6 accumulator
-// sets of 3 floats, bcf and bsh; then k_gather_planes' edge slots, or k_gather_runs' run offsets (2 pair
-// parities) and group bounds; the exact-path queues
-static size_t planes_fixed(int dtype, int cfg)
+static size_t planes_smem(int tch, int dtype)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
-    size_t f = 3 * slot + 64 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8;
-    if (exm_gather_cfg_sorted(cfg)) {
-        const size_t ng = (size_t)(kGatherCfgs[cfg].nw - 1) * (32 / EXM_RG);
-        f += 4 * (2 + 4 * (ng + 1)) + 16;   // offsets' +1 entries, the bounds, alignment of the queue
-    } else {
-        f += 2 * 2 * 8 * 32 * 4;
-    }
-    return f;
-}
-
-static size_t per_template_smem(int cfg) { return exm_gather_cfg_sorted(cfg) ? 22 * 4 : 20 * 4; }
-
-static size_t planes_smem(int tch, int dtype, int cfg)
-{
-    return planes_fixed(dtype, cfg) + (size_t)tch * per_template_smem(cfg);
+    // 6 accumulator sets of 3 floats, bcf, bsh; edge slots; exact-path queue counts and entries
+    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8;
 }
 
 // the most templates a block can hold in shared memory next to the staged planes
-static int planes_tch_max(exm_ctx *ctx, int cfg)
+static int planes_tch_max(exm_ctx *ctx)
 {
-    const size_t fixed = planes_fixed(ctx->dtype, cfg) + 2048;   // + static shared memory
+    const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
+    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 2048;   // + static
     const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
-    return (int)std::min<size_t>(EXM_TCH, room / per_template_smem(cfg) / 16 * 16);
+    return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
 
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc)
@@ -1316,15 +834,13 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     if (maxn <= 0) return;
     int tch = (int)((pairs + ctx->sm_count - 1) / ctx->sm_count);
     tch = (int)((long long)tch * ctx->gather_chunk_pct / 100);
-    const int cfg = (ctx->gather_cfg >= 0 && ctx->gather_cfg < kNumGatherCfgs) ? ctx->gather_cfg : 0;
-    if (exm_gather_cfg_sorted(cfg) != sl.desc_sorted)
-        EXM_THROW(EXM_ERR_STATE, "tap descriptors are not in the order of the chosen gather launch shape");
     tch = std::max(tch, 256);
-    tch = std::min(((tch + 15) / 16) * 16, planes_tch_max(ctx, cfg));
+    tch = std::min(((tch + 15) / 16) * 16, planes_tch_max(ctx));
     a.tch = tch;
     a.nch = (maxn + tch - 1) / tch;
-    const size_t smem = planes_smem(tch, ctx->dtype, cfg);
+    const size_t smem = planes_smem(tch, ctx->dtype);
     dim3 grid(rc * ctx->nn * a.nch);
+    const int cfg = (ctx->gather_cfg >= 0 && ctx->gather_cfg < kNumGatherCfgs) ? ctx->gather_cfg : 0;
     launch_cfg(ctx, cfg, a, grid, smem);
     EXM_CUDA(cudaGetLastError());
     // algorithmic work of this launch: one node-tap per (template slot, lag, walked time)

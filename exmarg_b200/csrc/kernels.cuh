@@ -181,7 +181,6 @@ struct ChunkInfo {
 void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc, bool first_chunk_of_lags);
 void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int rc);
 int exm_gather_num_cfgs();
-bool exm_gather_cfg_sorted(int cfg);
 void exm_run_node_lse(exm_ctx *ctx, exm_slot &sl, int m_base, int nmc);
 void exm_run_lnb(exm_ctx *ctx, exm_slot &sl);
 void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const int *d_rows, const int *d_tab,

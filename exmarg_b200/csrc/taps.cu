@@ -53,10 +53,9 @@ __device__ __forceinline__ void tap_time(const TapArgs &a, int i, int k, int &t,
 
 // the walked times of template i and their L samples, in shared memory when they fit
 struct WalkCache {
-    int *t;
+    int *t;        // the time, bit 31: a random draw
     float2 *l;
     float *llo;
-    int *flag;
     bool on;
 };
 
@@ -66,8 +65,7 @@ __device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 
     for (int k = threadIdx.x; k < a.nwalk; k += blockDim.x) {
         int t, flag;
         tap_time(a, i, k, t, flag);
-        wc.t[k] = t;
-        wc.flag[k] = flag;
+        wc.t[k] = (int)((unsigned)t | ((unsigned)flag << 31));
         wc.l[k] = L[t];
         wc.llo[k] = Llo[t];
     }
@@ -78,8 +76,9 @@ __device__ __forceinline__ void walk_at(const TapArgs &a, int i, const float2 *L
                                         int k, int &t, int &flag, float2 &l, float &llo)
 {
     if (wc.on) {
-        t = wc.t[k];
-        flag = wc.flag[k];
+        const int v = wc.t[k];
+        t = v & 0x7FFFFFFF;
+        flag = (unsigned)v >> 31;
         l = wc.l[k];
         llo = wc.llo[k];
     } else {
@@ -110,8 +109,7 @@ __global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
     wc.on = a.nwalk <= TAP_CACHE;
     wc.l = (float2 *)wsm;
     wc.t = (int *)(wc.l + TAP_CACHE);
-    wc.flag = wc.t + TAP_CACHE;
-    wc.llo = (float *)(wc.flag + TAP_CACHE);
+    wc.llo = (float *)(wc.t + TAP_CACHE);
     load_walk(a, i, L, Llo, wc);
     for (int rl = 0; rl < rc; ++rl) {
         for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) c[q] = 0;
@@ -206,8 +204,7 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     wc.on = a.nwalk <= TAP_CACHE;
     wc.l = (float2 *)wsm;
     wc.t = (int *)(wc.l + TAP_CACHE);
-    wc.flag = wc.t + TAP_CACHE;
-    wc.llo = (float *)(wc.flag + TAP_CACHE);
+    wc.llo = (float *)(wc.t + TAP_CACHE);
     load_walk(a, i, L, Llo, wc);
     const unsigned lt = (1u << lane) - 1u;
     const int C0 = a.win[0], Rh = a.win[1 + EXM_MAX_NODES];
@@ -360,7 +357,7 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     a.pitch = exm_desc_pitch(a.per_lag);
     if (first_chunk_of_lags) EXM_CUDA(cudaMemsetAsync(a.hist_b, 0, sizeof(int) * EXM_HB_N, ctx->stream));
     EXM_CUDA(cudaMemsetAsync(a.hist_d, 0, sizeof(int) * 256, ctx->stream));
-    const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + 2 * sizeof(int) + sizeof(float)) : 0;
+    const size_t wsm = a.nwalk <= TAP_CACHE ? (size_t)TAP_CACHE * (sizeof(float2) + sizeof(int) + sizeof(float)) : 0;
     exm_allow_smem(ctx, (const void *)k_tap_count, wsm);
     exm_allow_smem(ctx, (const void *)k_tap_scatter, wsm);
     a.win = (const int *)sl.win.p;
@@ -370,14 +367,9 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     k_windows<<<1, 256, 0, ctx->stream>>>(a.hist_b, a.hist_d, (const int *)ctx->d_cki.p, ctx->nn, ctx->nb, ctx->nd, ctx->ndp,
                                           exm_dtype_wd(ctx->dtype), exm_dtype_calign(ctx->dtype), (int *)sl.win.p);
     k_tap_scatter<<<ci.nmc, 256, wsm, ctx->stream>>>(a, rc);
-    // k_gather_planes reads lane-interleaved chunks, k_gather_runs the sorted order as scattered
-    sl.desc_sorted = exm_gather_cfg_sorted(ctx->gather_cfg);
-    if (!sl.desc_sorted) {
-        const long long n_chunks = (long long)rc * a.pitch / EXM_DCH;
-        k_tap_interleave<<<(int)std::min<long long>(n_chunks, (long long)ctx->sm_count * 32), 256, 0,
-                           ctx->stream>>>(a.desc, a.tside, n_chunks);
-        ctx->launches += 1;
-    }
+    const long long n_chunks = (long long)rc * a.pitch / EXM_DCH;
+    k_tap_interleave<<<(int)std::min<long long>(n_chunks, (long long)ctx->sm_count * 32), 256, 0, ctx->stream>>>(
+        a.desc, a.tside, n_chunks);
     EXM_CUDA(cudaGetLastError());
-    ctx->launches += 4;
+    ctx->launches += 5;
 }
