@@ -163,8 +163,7 @@ GATHER_TRAFFIC = {
     "sources_sha256": None,
     "capture": "profiles/k_gather_planes_small.md",
 }
-GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh",
-                  "exmarg_b200/csrc/common.cuh")
+GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh")
 
 
 def gather_sources_sha256():
@@ -342,6 +341,28 @@ def precision_legs(args, spec, s_nodes, rows, bank, store, store_h, gather_cfg, 
             if dt != "f32":
                 ctx.close()
         out[dt] = d
+    # float32 tables with the filter's ln|z| kept to float64 precision (filter_precision='fp64')
+    d = {}
+    try:
+        seg = make_inputs(args.warmup + args.prec_steps, 0, args.templates, args.nodes, args.lags)[2]
+        eb.pe_intrinsic(seg, bank, store, rows=[0], filter_precision="fp64")
+        bank.ctx.timing(True)
+        for i in range(args.warmup, args.warmup + args.prec_steps):
+            eb.pe_intrinsic(seg, bank, store, rows=[i], filter_precision="fp64")
+        tm = bank.ctx.timing(False)
+        d["segments_per_s"] = args.prec_steps / (tm["total_ms"] / 1000.0)
+        d["taps_ms"] = tm["taps_ms"] / args.prec_steps
+        errs, errs_ref = [], []
+        for sg, lb, lr in zip(segs, oracle, oracle_ref):
+            r = eb.pe_intrinsic(sg, bank, store, rows=[0], filter_precision="fp64")
+            v = restate.log_mean(r["ln_lambda"][0][idx], cell)
+            errs.append(abs(v - lb))
+            errs_ref.append(abs(v - lr))
+        d["abs_dlnB_per_snr"] = [float(x) for x in errs]
+        d["abs_dlnB_vs_reference_per_snr"] = [float(x) for x in errs_ref]
+    finally:
+        bank.ctx.set_filter_precision("reference")
+    out["f32_filter_fp64"] = d
     return out
 
 

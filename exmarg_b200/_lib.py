@@ -22,7 +22,7 @@ QUAD_GL64 = 16   # OR'ed into the prior: 64-point Gauss-Legendre distance quadra
 GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "32w x1", "32w x2")
 
 # every symbol include/exmarg_b200.h declares
-SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
+SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_set_filter_precision", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
            "exm_store_set_node", "exm_store_generate_node", "exm_store_get_node", "exm_bank_set", "exm_pe_prepare",
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
@@ -60,6 +60,7 @@ def load():
         "exm_ctx_set_graph": ([P, I], I),
         "exm_ctx_set_priority": ([P, I, P], I),
         "exm_ctx_test_wait_expiry": ([P, I], I),
+        "exm_ctx_set_filter_precision": ([P, I], I),
         "exm_last_error": ([P], ctypes.c_char_p),
         "exm_ctx_bytes": ([P], Z),
         "exm_ctx_timing": ([P, I, P], I),
@@ -149,6 +150,7 @@ class Context:
                 _raise(rc, share_store_of.lib.exm_last_error(share_store_of.h).decode())
             device = share_store_of.device
             self.parent = share_store_of            # keeps the store's owner alive
+            self.filter_precision = getattr(share_store_of, "filter_precision", "reference")   # inherited
         else:
             rc = self.lib.exm_ctx_create(int(device), int(hbm_budget), ctypes.byref(h))
             if rc != EXM_OK:
@@ -167,6 +169,16 @@ class Context:
     def set_graph(self, enable=True):
         """replay each segment's device work as one captured CUDA graph"""
         self._check(self.lib.exm_ctx_set_graph(self.h, 1 if enable else 0))
+
+    FILTER_PRECISIONS = ("reference", "fp64")
+
+    def set_filter_precision(self, precision):
+        """'reference' (ln|z| rounded to float32 as the reference leaves it) or 'fp64' (ln|z| kept to float64)"""
+        if precision not in self.FILTER_PRECISIONS:
+            raise ValueError("filter_precision must be 'reference' or 'fp64'")
+        if getattr(self, "filter_precision", "reference") != precision:
+            self._check(self.lib.exm_ctx_set_filter_precision(self.h, self.FILTER_PRECISIONS.index(precision)))
+            self.filter_precision = precision
 
     def test_wait_expiry(self, enable=True):
         """test support: the plane gather stages nothing, so its bounded waits run out (EXM_ERR_TIMEOUT)"""

@@ -302,6 +302,7 @@ extern "C" int exm_ctx_create_sharing(exm_ctx *parent, size_t hbm_budget, exm_ct
         ctx->tmap_ok = parent->tmap_ok;
         ctx->gather_cfg = parent->gather_cfg;
         ctx->gather_chunk_pct = parent->gather_chunk_pct;
+        ctx->traj_fp64 = parent->traj_fp64;
         exm_ensure(ctx, ctx->d_stats, 4 * sizeof(unsigned long long));
         EXM_CUDA(cudaMemset(ctx->d_stats.p, 0, 4 * sizeof(unsigned long long)));
     } catch (const exm_error &e) {
@@ -868,7 +869,7 @@ static void ensure_slot(exm_ctx *ctx, exm_slot &sl, const RunShape &rs)
 {
     const size_t nmc = rs.nmc_max, nt = ctx->nt, nf = ctx->nfreq;
     exm_ensure(ctx, sl.traj, 2 * nmc * nt * sizeof(float2));
-    exm_ensure(ctx, sl.trajlo, 2 * nmc * nt * sizeof(float));
+    if (ctx->traj_fp64) exm_ensure(ctx, sl.trajlo, 2 * nmc * nt * sizeof(float));
     exm_ensure(ctx, sl.fft, 2 * nmc * nt * sizeof(double2));
     const size_t n_draws = rs.K > 0 ? (((size_t)ctx->nm * rs.S + EXM_MAX_REJ + 63) / 64) * 64 : 0;
     exm_ensure(ctx, sl.keys, std::max<size_t>(rs.K > 0 ? nmc * nt : 1, n_draws) * sizeof(uint32_t));
@@ -1241,7 +1242,8 @@ extern "C" int exm_set_trajectories(exm_ctx *ctx, const float *traj)
             for (size_t t = 0; t < nt; ++t) dst[t] = make_float2(lq[t], ph[t]);
         }
     EXM_CUDA(cudaMemcpy(sl.traj.p, h.data(), sizeof(float2) * h.size(), cudaMemcpyHostToDevice));
-    EXM_CUDA(cudaMemset(sl.trajlo.p, 0, sizeof(float) * h.size()));   // float32 trajectories: no residual
+    if (sl.trajlo.p)   // float32 trajectories: no residual
+        EXM_CUDA(cudaMemset(sl.trajlo.p, 0, std::min(sl.trajlo.bytes, sizeof(float) * h.size())));
     ctx->traj_ok = true;
     ctx->times_ok = false;
     ctx->cur_nwalk = ctx->nt;
@@ -1282,6 +1284,17 @@ extern "C" int exm_select_times(exm_ctx *ctx, int64_t seed, int n_loud, int n_ra
             }
         }
     }
+    API_END(ctx)
+}
+
+extern "C" int exm_ctx_set_filter_precision(exm_ctx *ctx, int mode)
+{
+    API_BEGIN(ctx)
+    REQUIRE(mode == EXM_FILTER_REFERENCE || mode == EXM_FILTER_FP64, EXM_ERR_ARG,
+            "filter precision is EXM_FILTER_REFERENCE or EXM_FILTER_FP64");
+    ctx->traj_fp64 = mode == EXM_FILTER_FP64;
+    ctx->traj_ok = ctx->times_ok = false;   // trajectories of the other precision are not reused
+    ctx->graph_key[0] = -1;
     API_END(ctx)
 }
 

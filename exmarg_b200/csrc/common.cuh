@@ -54,7 +54,7 @@ struct dbuf {
 // per-segment workspace of the analysis pipeline
 struct exm_slot {
     dbuf traj;      // float2 [2][nm][nt]: (ln|z|, arg z) of H then L
-    dbuf trajlo;    // float [2][nm][nt]: ln|z| - float(ln|z|) (0 for trajectories uploaded as float32)
+    dbuf trajlo;    // float [2][nm][nt]: ln|z| - float(ln|z|), filter precision 'fp64' only (0 for uploaded trajectories)
     dbuf fft;       // double2 [2][nm][nt]: the padded rows and their transforms
     dbuf keys;      // uint32 [nm][nt]: selection scores as ordered integers
     dbuf picks;     // int32 [nm][S]: random ranks into the rest
@@ -133,6 +133,7 @@ struct exm_ctx {
     int gather_cfg = 0;
     int gather_chunk_pct = 100;
     bool test_wait_expiry = false;
+    bool traj_fp64 = false;          // filter precision 'fp64': the ln|z| residual is kept and used by the taps
     exm_server *srv = nullptr;       // request loop served from this context (exm_serve_start)   // the plane gather stages nothing and its barrier waits run out (a test)   // templates per gather block, percent of the one-wave-per-lag size
 
     // cuFFT

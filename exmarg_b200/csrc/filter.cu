@@ -2,9 +2,10 @@
 //   w_I = complex64(conj(d_I) / sig2_I)          (float64 division, rounded once)
 //   pad[m, lo:lo+nf] = W[m] * w_I                 (complex64 product, no FMA contraction)
 //   z = FFT_forward(pad)                          (cuFFT Z2Z, length n_time, batched)
-//   (ln|z|, arg z) = (0.5 ln max(re^2 + im^2, 1e-38), atan2(im, re)), rounded once to float32, and the
-//   float32 residual ln|z| - float(ln|z|) beside them (the tap geometry adds it back: ln|z| rounded to float32
-//   alone moves loud taps by ~1e-5 in ln Lambda through the table slopes)
+//   (ln|z|, arg z) = (0.5 ln max(re^2 + im^2, 1e-38), atan2(im, re)), rounded once to float32 as the
+//   reference rounds them; with filter precision 'fp64' also the float32 residual ln|z| - float(ln|z|), which
+//   the tap geometry adds back (the float32 rounding of ln|z| moves loud taps by ~1e-5 in ln Lambda through the
+//   table slopes, in the reference as here)
 // The complex64 product (the reference's pad) is transformed in float64, so each
 // trajectory sample is the float32 rounding of the exact filter output of that pad:
 // a float32 FFT adds its own rounding (cuFFT's is several times larger than numpy's),
@@ -45,7 +46,7 @@ __global__ void k_premul(const float2 *__restrict__ W, const float2 *__restrict_
     pad[idx] = o;
 }
 
-// z (float64) -> (ln|z|, arg z) float32 and the residual of ln|z|
+// z (float64) -> (ln|z|, arg z) float32 and, if lo is not null, the residual of ln|z|
 __global__ void k_polar(const double2 *__restrict__ z, float2 *__restrict__ out, float *__restrict__ lo, long long n)
 {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -56,7 +57,7 @@ __global__ void k_polar(const double2 *__restrict__ z, float2 *__restrict__ out,
         const double lq = 0.5 * log(fmax(p, 1e-38));
         const float hi = (float)lq;
         out[i] = make_float2(hi, (float)atan2(v.y, v.x));
-        lo[i] = (float)(lq - (double)hi);
+        if (lo) lo[i] = (float)(lq - (double)hi);
     }
 }
 
@@ -72,7 +73,8 @@ void exm_run_filter(exm_ctx *ctx, exm_slot &sl, const float2 *dW, int nm)
     EXM_CUDA(cudaGetLastError());
     exm_fft_plan(ctx, 2 * nm);
     EXM_CUFFT(cufftExecZ2Z(ctx->plan, (cufftDoubleComplex *)z, (cufftDoubleComplex *)z, CUFFT_FORWARD));
-    k_polar<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(z, traj, (float *)sl.trajlo.p, total);
+    k_polar<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(z, traj, ctx->traj_fp64 ? (float *)sl.trajlo.p : nullptr,
+                                                         total);
     EXM_CUDA(cudaGetLastError());
     ctx->launches += 3;
 }

@@ -38,7 +38,7 @@ struct PlaneArgs {
     const int32_t *tside;
     const int *off;
     const float2 *H, *L;
-    const float *Hlo, *Llo;      // residuals of ln|z| (zeros for uploaded float32 trajectories)
+    const float *Hlo, *Llo;      // residuals of ln|z| (filter precision 'fp64'), else null
     const void *T;               // node tables, element type of the kernel's TE
     const int *mlo, *mhi, *bnode, *win, *tau;
     const double *boff, *cb, *ckd;
@@ -240,8 +240,9 @@ __device__ EXM_SLOW_INLINE double slow_tap(const PlaneArgs &a, int il, int tm, i
     if (i1 >= nt) i1 -= nt;
     const int gi = il + m_base;
     const double offb = (BND ? a.cb[gi] : a.ckd[k]) + a.boff[gi];   // ckd: (ln s_k - beta0)/dbeta
-    return exm_tap_fp64<TE>(a.L[(long long)il * nt + tm], a.H[(long long)il * nt + i1], a.Llo[(long long)il * nt + tm],
-                            a.Hlo[(long long)il * nt + i1], offb, r,
+    return exm_tap_fp64<TE>(a.L[(long long)il * nt + tm], a.H[(long long)il * nt + i1],
+                            a.Llo ? a.Llo[(long long)il * nt + tm] : 0.f, a.Hlo ? a.Hlo[(long long)il * nt + i1] : 0.f,
+                            offb, r,
                             (const TE *)a.T + (long long)k * a.tstride, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
                             a.rdd, a.offd);
 }
@@ -782,8 +783,8 @@ void exm_run_gather_planes(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int 
     a.off = (const int *)sl.cnt.p;
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ci.nmc * ctx->nt;
-    a.Hlo = (const float *)sl.trajlo.p;
-    a.Llo = a.Hlo + (size_t)ci.nmc * ctx->nt;
+    a.Hlo = ctx->traj_fp64 ? (const float *)sl.trajlo.p : nullptr;
+    a.Llo = a.Hlo ? a.Hlo + (size_t)ci.nmc * ctx->nt : nullptr;
     a.T = ctx->T.p;
     a.mlo = (const int *)ctx->d_mlo.p;
     a.mhi = (const int *)ctx->d_mhi.p;
@@ -882,7 +883,7 @@ __global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
     const int nt = a.nt;
     const int tau0 = ((a.tau[r] % nt) + nt) % nt;
     const float2 *H = a.H + (long long)row * nt, *L = a.L + (long long)row * nt;
-    const float *Hlo = a.Hlo + (long long)row * nt, *Llo = a.Llo + (long long)row * nt;
+    const float *Hlo = a.Hlo ? a.Hlo + (long long)row * nt : nullptr, *Llo = a.Llo ? a.Llo + (long long)row * nt : nullptr;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int n = 0; n < a.ns; ++n) {
         const int tb = a.tab[j * a.ns + n];
@@ -899,7 +900,7 @@ __global__ void __launch_bounds__(256) k_gather_simple(SimpleArgs a)
             }
             int i1 = t + tau0;
             if (i1 >= nt) i1 -= nt;
-            double acc = exm_tap_fp64<TE>(L[t], H[i1], Llo[t], Hlo[i1], offb, r, Tn, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
+            double acc = exm_tap_fp64<TE>(L[t], H[i1], Llo ? Llo[t] : 0.f, Hlo ? Hlo[i1] : 0.f, offb, r, Tn, sc, a.nphif, a.nb, a.nd, a.ndp, a.rph, a.rdb,
                                           a.rdd, a.offd);
             if (a.use_sel) acc += flag ? (double)a.lw : 0.0;
             if (acc > m) {
@@ -963,8 +964,8 @@ void exm_run_gather_simple(exm_ctx *ctx, exm_slot &sl, int nsel, int ns, const i
     SimpleArgs a;
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ctx->nm * ctx->nt;
-    a.Hlo = (const float *)sl.trajlo.p;
-    a.Llo = a.Hlo + (size_t)ctx->nm * ctx->nt;
+    a.Hlo = ctx->traj_fp64 ? (const float *)sl.trajlo.p : nullptr;
+    a.Llo = a.Hlo ? a.Hlo + (size_t)ctx->nm * ctx->nt : nullptr;
     a.sel = (const int32_t *)sl.sel.p;
     a.T = ctx->T.p;
     a.tsc = (const float *)ctx->d_tscale.p;

@@ -20,7 +20,7 @@
 
 struct TapArgs {
     const float2 *H, *L;
-    const float *Hlo, *Llo;   // residuals of ln|z| (filter output) or zeros
+    const float *Hlo, *Llo;   // residuals of ln|z| (filter precision 'fp64'), else null
     const int32_t *sel;
     const double *boff;   // [nmc] -ln(u)/dbeta of the chunk's templates
     const int *tau;       // [ntau]
@@ -67,7 +67,7 @@ __device__ __forceinline__ void load_walk(const TapArgs &a, int i, const float2 
         tap_time(a, i, k, t, flag);
         wc.t[k] = (int)((unsigned)t | ((unsigned)flag << 31));
         wc.l[k] = L[t];
-        wc.llo[k] = Llo[t];
+        wc.llo[k] = Llo ? Llo[t] : 0.f;
     }
     __syncthreads();
 }
@@ -84,7 +84,7 @@ __device__ __forceinline__ void walk_at(const TapArgs &a, int i, const float2 *L
     } else {
         tap_time(a, i, k, t, flag);
         l = L[t];
-        llo = Llo[t];
+        llo = Llo ? Llo[t] : 0.f;
     }
 }
 
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
         for (int q = threadIdx.x; q < EXM_HB_N; q += blockDim.x) hb[q] = 0;
     const int nt = a.g.nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
-    const float *Hlo = a.Hlo + (long long)i * nt, *Llo = a.Llo + (long long)i * nt;
+    const float *Hlo = a.Hlo ? a.Hlo + (long long)i * nt : nullptr, *Llo = a.Llo ? a.Llo + (long long)i * nt : nullptr;
     const double boff = a.boff[i];
     WalkCache wc;
     wc.on = a.nwalk <= TAP_CACHE;
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) k_tap_count(TapArgs a, int rc)
             if (i1 >= nt) i1 -= nt;
             int p, ib, d0;
             float w, fb, fd;
-            exm_tap_geom(l, H[i1], llo, Hlo[i1], boff, a.g, p, w, ib, fb, d0, fd);
+            exm_tap_geom(l, H[i1], llo, Hlo ? Hlo[i1] : 0.f, boff, a.g, p, w, ib, fb, d0, fd);
             // warp-aggregated increments: one atomic per distinct bin in the warp
             const unsigned pm = __match_any_sync(__activemask(), p);
             if ((threadIdx.x & 31) == __ffs(pm) - 1) atomicAdd(&c[p], __popc(pm));
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nt = a.g.nt;
     const float2 *H = a.H + (long long)i * nt, *L = a.L + (long long)i * nt;
-    const float *Hlo = a.Hlo + (long long)i * nt, *Llo = a.Llo + (long long)i * nt;
+    const float *Hlo = a.Hlo ? a.Hlo + (long long)i * nt : nullptr, *Llo = a.Llo ? a.Llo + (long long)i * nt : nullptr;
     const double boff = a.boff[i];
     WalkCache wc;
     wc.on = a.nwalk <= TAP_CACHE;
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
                 walk_at(a, i, L, Llo, wc, k, t, flag, l, llo);
                 int i1 = t + tau0;
                 if (i1 >= nt) i1 -= nt;
-                exm_tap_geom(l, H[i1], llo, Hlo[i1], boff, a.g, p, w, ib, fb, d0, fd);
+                exm_tap_geom(l, H[i1], llo, Hlo ? Hlo[i1] : 0.f, boff, a.g, p, w, ib, fb, d0, fd);
             }
             const unsigned peers = __match_any_sync(0xffffffffu, p);
             const int rk = __popc(peers & lt);
@@ -332,8 +332,8 @@ void exm_run_taps(exm_ctx *ctx, exm_slot &sl, const ChunkInfo &ci, int r0, int r
     TapArgs a;
     a.H = (const float2 *)sl.traj.p;
     a.L = a.H + (size_t)ci.nmc * nt;
-    a.Hlo = (const float *)sl.trajlo.p;
-    a.Llo = a.Hlo + (size_t)ci.nmc * nt;
+    a.Hlo = ctx->traj_fp64 ? (const float *)sl.trajlo.p : nullptr;
+    a.Llo = a.Hlo ? a.Hlo + (size_t)ci.nmc * nt : nullptr;
     a.sel = (const int32_t *)sl.sel.p;
     a.boff = (const double *)ctx->d_bhat_off.p + ci.m_base;
     a.tau = (const int *)ctx->d_tau.p;

@@ -55,9 +55,13 @@ def prepare(bank, store, prior="volume", ymin=0.1267, quadrature="reference"):
 
 
 def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, chunk=4, nodes_per_launch=6,
-                 block=256, resident=False, n_loud=1024, n_random=1024, seed=0, quadrature="reference"):
+                 block=256, resident=False, n_loud=1024, n_random=1024, seed=0, quadrature="reference",
+                 filter_precision="reference"):
     """ln Lambda of each template of the bank, the distance integrated over its prior.
     quadrature ('b200' only): 'reference' (the reference's rules) or 'gl64' (see prepare).
+    filter_precision ('b200' only): 'reference' -- ln|z| rounded to float32 as the reference's filter leaves it,
+    so results follow the reference's; 'fp64' -- ln|z| kept to float64 precision, so results follow the
+    float64 evaluation (at high SNR the reference's float32 rounding moves ln B by up to ~1e-4)
 
     returns dict: M, q, chi, u (n_template,), ln_lambda (n_segment, n_template),
     ln_b (n_segment,), rows."""
@@ -72,6 +76,7 @@ def pe_intrinsic(segments, bank, store, rows=None, prior="volume", ymin=0.1267, 
         raise ValueError("chunk and nodes_per_launch must be >= 1")
     seg = read_segments(segments, rows)
     ctx = prepare(bank, store, prior, ymin, quadrature)
+    ctx.set_filter_precision(filter_precision)
     seeds = seed + np.asarray(seg["rows"], np.int64)
     apply_tuned(ctx, n_loud, n_random)
     lnl, lnb = ctx.pe_intrinsic(seg["d_H"], seg["d_L"], seg["sig2_H"], seg["sig2_L"], seeds, n_loud, n_random)

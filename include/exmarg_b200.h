@@ -80,6 +80,17 @@ EXM_API int exm_ctx_set_graph(exm_ctx *ctx, int enable);
 EXM_API int exm_ctx_set_priority(exm_ctx *ctx, int priority, int *range_out);
 EXM_API const char *exm_last_error(const exm_ctx *ctx);
 
+/* Precision of the trajectories the table reads see.  EXM_FILTER_REFERENCE (the default): ln|z| and arg z
+ * rounded once to float32, as the reference's filter leaves them (exmarg/search/bank.py:74-75); results
+ * follow the reference's, float32 rounding included (at SNR 30-50 that rounding moves the reference's ln B
+ * by 3e-5-7e-5 from float64).  EXM_FILTER_FP64: the float64 filter's ln|z| is kept to float64 precision (a
+ * float32 residual beside the float32 value), so ln B follows float64 instead (within ~1e-5 at SNR 50); it
+ * costs one more load per tap in the tap build and 4 bytes per trajectory sample.  No reference
+ * counterpart. */
+#define EXM_FILTER_REFERENCE 0
+#define EXM_FILTER_FP64 1
+EXM_API int exm_ctx_set_filter_precision(exm_ctx *ctx, int mode);
+
 /* Test support for failure detection (no reference counterpart).  enable = 1: the plane gather of
  * this context issues no table copy, so its first bounded barrier wait runs out (after ~20k cycles
  * instead of ~1 s); the kernel then sets the device error word and returns, and the call fails with
