@@ -158,9 +158,9 @@ def measured_peaks():
 # read per node-tap both do), so the full launch's traffic is this figure times its node-taps.  The capture
 # holds only for the kernel sources it was taken on: if they changed since, traffic is reported as null.
 GATHER_TRAFFIC = {
-    "dram_bytes_per_node_tap": None,
-    "l2_read_hit_rate": None,
-    "sources_sha256": None,
+    "dram_bytes_per_node_tap": 3.9162,       # (1.8548e9 + 6.56e6) B / 4.7531e8 node-taps
+    "l2_read_hit_rate": 74.76,             # lts__t_sector_op_read_hit_rate.pct
+    "sources_sha256": "4c82d786e83b07ebf753fc1e6c307772303e922a79a6a8cc46ee6d9ed4172f99",
     "capture": "profiles/k_gather_planes_small.md",
 }
 GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh")
@@ -836,9 +836,11 @@ def serve_config_leg(args, store, local):
     n_cap, n_poi = args.serve_capacity_requests, args.serve_poisson_requests
     mix = [(keys[int(rng.choice(len(keys), p=weights))], int(rng.integers(0, 16))) for _ in range(n_cap + n_poi)]
     free0, total0 = eb.device_memory(local)
-    ctx.serve_start(hbm_budget=0, max_workers=args.serve_workers, n_loud=N_LOUD, n_random=N_RANDOM, graph=True)
+    budget = int(args.serve_budget_gb * 1e9) if args.serve_budget_gb > 0 else 0
+    ctx.serve_start(hbm_budget=budget, max_workers=args.serve_config_workers, n_loud=N_LOUD, n_random=N_RANDOM,
+                    graph=True)
     out = {"banks": {k: {"templates": nm, "segment_s": T} for k, nm, T in SERVE_BANKS},
-           "mix_weights": weights.tolist(), "snr": "U(0, 50), 90% noise-only", "workers_max": args.serve_workers}
+           "mix_weights": weights.tolist(), "snr": "U(0, 50), 90% noise-only", "workers_max": args.serve_config_workers}
     try:
         ids = {k: ctx.serve_add_bank(b.W, b.lo, b.n_time, b.u, b.M, b.q, b.chi, 0.1267) for k, b in banks.items()}
         stats0 = ctx.serve_stats()
@@ -1095,6 +1097,9 @@ def main():
     ap.add_argument("--serve-capacity-requests", type=int, default=200, help="requests queued at once (capacity)")
     ap.add_argument("--serve-poisson-requests", type=int, default=1000, help="requests of the Poisson stream")
     ap.add_argument("--serve-load", type=float, default=0.8, help="Poisson rate as a fraction of the capacity")
+    ap.add_argument("--serve-budget-gb", type=float, default=60.0,
+                    help="workspace budget of the serving-config leg's workers, GB (0: 85%% of free memory)")
+    ap.add_argument("--serve-config-workers", type=int, default=4, help="worker limit of the serving-config leg")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
