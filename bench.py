@@ -821,7 +821,7 @@ def serve_config_leg(args, store, local):
     (the config's 400 req/s is stated beside it as a multiple of the capacity).  Latency is arrival to result
     (p50 / p99); a sample of served results is compared bitwise with the plain single-segment path."""
     import exmarg_b200 as eb
-    from exmarg_b200 import synth
+    from exmarg_b200 import _lib, synth
     ctx = eb.context(local)
     rng = np.random.default_rng(2027)
     banks, segs = {}, {}
@@ -835,7 +835,7 @@ def serve_config_leg(args, store, local):
     weights = np.array([0.2, 0.2, 0.2, 0.15, 0.15, 0.1])
     n_cap, n_poi = args.serve_capacity_requests, args.serve_poisson_requests
     mix = [(keys[int(rng.choice(len(keys), p=weights))], int(rng.integers(0, 16))) for _ in range(n_cap + n_poi)]
-    free0, total0 = eb.device_memory(local)
+    free0, total0 = _lib.device_memory(local)
     budget = int(args.serve_budget_gb * 1e9) if args.serve_budget_gb > 0 else 0
     ctx.serve_start(hbm_budget=budget, max_workers=args.serve_config_workers, n_loud=N_LOUD, n_random=N_RANDOM,
                     graph=True)
