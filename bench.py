@@ -851,14 +851,18 @@ def serve_config_leg(args, store, local):
             return ctx.submit(ids[key], sg["d_H"][e], sg["d_L"][e], sg["sig2_H"], sg["sig2_L"], e)
 
         # warm-up: one request per bank (opens workers, plans, graphs)
+        t_w = time.perf_counter()
         for k in keys:
             ctx.poll(submit(k, 0), banks[k].u.size)
+        out["warmup_s"] = time.perf_counter() - t_w
+        print("serve-config: workers open (%.1f s)" % out["warmup_s"], file=sys.stderr, flush=True)
         # capacity: everything queued at once
         t0 = time.perf_counter()
         hs = [(submit(k, e), k, e) for k, e in mix[:n_cap]]
         served = [(ctx.poll(h, banks[k].u.size), k, e) for h, k, e in hs]
         cap = n_cap / (time.perf_counter() - t0)
         out["capacity"] = {"requests": n_cap, "segments_per_s": cap}
+        print("serve-config: capacity %.2f segments/s" % cap, file=sys.stderr, flush=True)
         # the Poisson stream at a stated fraction of that capacity
         rate = args.serve_load * cap
         arrivals = np.cumsum(rng.exponential(1.0 / rate, n_poi))
@@ -867,6 +871,9 @@ def serve_config_leg(args, store, local):
         i = 0
         while i < n_poi or pend:
             now = time.perf_counter() - t0
+            if now > args.serve_max_s and i < n_poi:        # a wall-clock guard: stop offering, drain
+                n_poi = i
+                print("serve-config: stream cut at %d requests after %.0f s" % (i, now), file=sys.stderr, flush=True)
             while i < n_poi and arrivals[i] <= now:
                 k, e = mix[n_cap + i]
                 pend[submit(k, e)] = (k, arrivals[i])
@@ -882,7 +889,7 @@ def serve_config_leg(args, store, local):
             time.sleep(0.0005)
         st = ctx.serve_stats()
         lat = np.array(lat)
-        out["poisson"] = {"requests": n_poi, "offered_per_s": rate, "offered_fraction_of_capacity": args.serve_load,
+        out["poisson"] = {"requests": n_poi, "requests_planned": args.serve_poisson_requests, "offered_per_s": rate, "offered_fraction_of_capacity": args.serve_load,
                           "segments_per_s": n_poi / (max(done_t) - arrivals[0]),
                           "latency_ms_p50": float(np.percentile(lat, 50) * 1e3),
                           "latency_ms_p99": float(np.percentile(lat, 99) * 1e3),
@@ -1097,9 +1104,11 @@ def main():
     ap.add_argument("--serve-capacity-requests", type=int, default=200, help="requests queued at once (capacity)")
     ap.add_argument("--serve-poisson-requests", type=int, default=1000, help="requests of the Poisson stream")
     ap.add_argument("--serve-load", type=float, default=0.8, help="Poisson rate as a fraction of the capacity")
-    ap.add_argument("--serve-budget-gb", type=float, default=60.0,
+    ap.add_argument("--serve-budget-gb", type=float, default=0.0,
                     help="workspace budget of the serving-config leg's workers, GB (0: 85%% of free memory)")
-    ap.add_argument("--serve-config-workers", type=int, default=4, help="worker limit of the serving-config leg")
+    ap.add_argument("--serve-config-workers", type=int, default=6, help="worker limit of the serving-config leg")
+    ap.add_argument("--serve-max-s", type=float, default=600.0,
+                    help="wall-clock limit of the serving-config leg's Poisson stream, s (then it drains)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
