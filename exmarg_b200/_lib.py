@@ -27,7 +27,7 @@ SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_
            "exm_pe_intrinsic", "exm_filter", "exm_set_trajectories", "exm_select_times", "exm_np_exp32", "exm_set_times",
            "exm_gather", "exm_node_values", "exm_gather_noalloc", "exm_autotune", "exm_set_gather_cfg",
            "exm_redshift_grid", "exm_source_frame", "exm_serve_start", "exm_serve_add_bank", "exm_submit", "exm_poll",
-           "exm_serve_stats", "exm_serve_stop", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
+           "exm_serve_stats", "exm_serve_stop", "exm_serve_set_min_idle", "exm_store_load", "exm_store_set_shard", "exm_bd_build", "exm_w_build", "exm_k_edges")
 
 LOAD_DIRECT = 1
 LOAD_STATS = ("seconds", "file_bytes", "host_bytes", "direct_nodes", "buffers", "chunk_bytes", "read_seconds",
@@ -88,6 +88,7 @@ def load():
         "exm_poll": ([P, ctypes.c_int64, ctypes.c_int64, P, P], I),
         "exm_serve_stats": ([P, P], I),
         "exm_serve_stop": ([P], I),
+        "exm_serve_set_min_idle": ([P, D], I),
         "exm_source_frame": ([P, P, P, P], I),
         "exm_store_load": ([P, I, I, P, P, P, P, P, P, I, ctypes.c_longlong, I, P], I),
         "exm_store_set_shard": ([P, D], I),
@@ -461,6 +462,10 @@ class Context:
         out = np.zeros(len(self.SERVE_STATS), np.float64)
         self._check(self.lib.exm_serve_stats(self.h, _p(out)))
         return dict(zip(self.SERVE_STATS, out.tolist()))
+
+    def serve_set_min_idle(self, seconds):
+        """an idle worker is closed for another bank only after `seconds` idle (default 0.25)"""
+        self._check(self.lib.exm_serve_set_min_idle(self.h, float(seconds)))
 
     def serve_stop(self):
         self._check(self.lib.exm_serve_stop(self.h))

@@ -11,8 +11,11 @@
 //   idle worker of its bank starts on it; else, if its bank has no worker at all, idle workers of banks with
 //   no queued request are closed until a new worker fits the HBM budget and the worker limit; a bank whose
 //   workers are all busy gets another only from free budget (opening a worker -- context, workspace, FFT
-//   plans, graph capture -- costs more than a segment).  A worker's cost is first estimated from its bank's
-//   shape and replaced by the bytes its context holds after its first segment;
+//   plans, graph capture -- costs more than a segment).  Only a worker idle for at least the server's
+//   minimum idle time (0.25 s by default) may be closed, so a mix of banks wider than the budget does not
+//   close and reopen workers on every bank change; a dispatcher thread re-runs admission every 20 ms while
+//   requests wait.  A worker's cost is first estimated from its bank's shape and replaced by the bytes its
+//   context holds after its first segment;
 // * a request that starts while r others run gets the r-th highest stream priority, so the oldest
 //   segment's gather leads and the others fill its gaps;
 // * every worker takes the parent's gather launch shape, so a result is bitwise the result of
@@ -59,6 +62,7 @@ struct SrvWorker {
     std::condition_variable cv;
     std::shared_ptr<SrvRequest> job;
     int rank = 0;           // requests already on the device when the job was assigned
+    double t_idle = 0.0;    // when the worker last became idle
     bool stop = false;
     bool waiting = false;   // parked on cv: the only state in which another thread may close it
 };
@@ -84,7 +88,10 @@ struct exm_server {
     int next_worker = 0, n_running = 0;
     long long n_served = 0, n_failed = 0, n_created = 0, n_evicted = 0;
     double t_first = 0.0, t_last = 0.0;
+    double min_idle_s = 0.25;          // an idle worker is closed for another bank only after this long
     bool stopping = false;
+    std::condition_variable cv_disp;   // wakes the dispatcher when requests are queued
+    std::thread dispatcher;
 };
 
 // device bytes one worker's workspace takes for a bank (as exm_pe_intrinsic sizes it): the FFT rows and
@@ -128,6 +135,7 @@ static std::unique_ptr<SrvWorker> evict_one(exm_server *s, int need)
     for (auto it = s->workers.begin(); it != s->workers.end(); ++it) {
         SrvWorker *w = it->second.get();
         if (w->bank == need || waiting[w->bank] || w->job || !w->waiting) continue;
+        if (now_s() - w->t_idle < s->min_idle_s) continue;   // recently used: keep it
         std::unique_ptr<SrvWorker> out = std::move(it->second);
         s->workers.erase(it);
         s->used -= std::min(s->used, s->banks[out->bank].cost);
@@ -239,6 +247,7 @@ static void worker_main(exm_server *s, SrvWorker *w)
         r->lnb = lnb;
         finish(s, *r, rc2, msg);
         w->job.reset();
+        w->t_idle = now_s();
         SrvBank &b = s->banks[w->bank];
         if (rc2 == EXM_OK && !b.measured) {   // the estimate gives way to the measured size
             size_t n_of_bank = 0;
@@ -272,6 +281,24 @@ static void worker_main(exm_server *s, SrvWorker *w)
     lk.unlock();
     if (w->ctx) exm_ctx_destroy(w->ctx);
     w->ctx = nullptr;
+}
+
+// re-runs admission while requests are queued (a closing rule may hold them until a worker has idled long
+// enough, with no submit or finish to trigger admission again)
+static void dispatcher_main(exm_server *s)
+{
+    std::unique_lock<std::mutex> lk(s->mu);
+    while (!s->stopping) {
+        s->cv_disp.wait_for(lk, std::chrono::milliseconds(20), [&] { return s->stopping; });
+        if (s->stopping || s->queue.empty()) continue;
+        std::vector<std::unique_ptr<SrvWorker>> closed;
+        admit(s, closed);
+        if (!closed.empty()) {
+            lk.unlock();
+            join_closed(closed);
+            lk.lock();
+        }
+    }
 }
 
 #define SRV_BEGIN(ctx)                                                                                             \
@@ -315,6 +342,7 @@ extern "C" int exm_serve_start(exm_ctx *ctx, size_t hbm_budget, int max_workers,
     s->n_loud = n_loud;
     s->n_random = n_random;
     s->graph = use_graph ? 1 : 0;
+    s->dispatcher = std::thread(dispatcher_main, s.get());
     ctx->srv = s.release();
     SRV_END(ctx)
 }
@@ -447,6 +475,7 @@ void exm_serve_destroy(exm_ctx *ctx)
     {
         std::unique_lock<std::mutex> lk(s->mu);
         s->stopping = true;
+        s->cv_disp.notify_all();
         for (auto &r : s->queue) finish(s, *r, EXM_ERR_STATE, "the server stopped before the request started");
         s->queue.clear();
         s->cv_done.wait(lk, [&] { return s->n_running == 0; });
@@ -458,9 +487,21 @@ void exm_serve_destroy(exm_ctx *ctx)
         s->workers.clear();
         s->cv_done.notify_all();
     }
+    if (s->dispatcher.joinable()) s->dispatcher.join();
     join_closed(all);
     ctx->srv = nullptr;
     delete s;
+}
+
+extern "C" int exm_serve_set_min_idle(exm_ctx *ctx, double seconds)
+{
+    SRV_BEGIN(ctx)
+    exm_server *s = ctx->srv;
+    if (!s) EXM_THROW(EXM_ERR_STATE, "no server on this context (exm_serve_start)");
+    if (!(seconds >= 0.0 && seconds <= 3600.0)) EXM_THROW(EXM_ERR_ARG, "minimum idle time must be 0..3600 s");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->min_idle_s = seconds;
+    SRV_END(ctx)
 }
 
 extern "C" int exm_serve_stop(exm_ctx *ctx)

@@ -307,6 +307,12 @@ EXM_API int exm_submit(exm_ctx *ctx, int bank_id, const double *d_H, const doubl
  * (message in exm_last_error) and the handle is released.  Safe to call from several host threads. */
 EXM_API int exm_poll(exm_ctx *ctx, int64_t handle, int64_t timeout_us, double *ln_lambda, double *ln_b);
 
+/* An idle worker is closed to make room for another bank only after it has been idle for `seconds` (default
+ * 0.25; 0: at once).  With a mix of banks whose workers do not fit the budget together, closing at once turns
+ * every bank change into a close and an open (seconds each); the minimum idle time bounds that churn, and the
+ * request of a bank without a worker waits for a worker to qualify.  No reference counterpart. */
+EXM_API int exm_serve_set_min_idle(exm_ctx *ctx, double seconds);
+
 /* Server counters, out (10 doubles): requests served, failed, queued, running; workers open, opened in
  * all, closed for budget; workspace bytes in use (estimated or measured), the budget; seconds from the
  * first request of an idle server to the last result. */

@@ -102,3 +102,25 @@ def test_serve_errors():
     r = eb.pe_intrinsic(fx.seg, banks["big"], fx.store, prior=fx.prior_arg, ymin=fx.ymin, n_loud=fx.n_loud,
                         n_random=fx.n_random, seed=0)
     assert np.abs(r["ln_b"] - fx.ln_b).max() <= 1e-5
+
+
+def test_minimum_idle_time_before_closing_a_worker():
+    # one worker slot: bank 'small' needs the slot bank 'big' holds; the big worker was just used, so it is not
+    # closed at once (stats after 0.3 s) but once it has been idle for the minimum idle time (1 s)
+    fx, ctx, banks, seg = _setup()
+    ctx.serve_start(hbm_budget=0, max_workers=1, n_loud=fx.n_loud, n_random=fx.n_random)
+    try:
+        ctx.serve_set_min_idle(1.0)
+        ids = {k: ctx.serve_add_bank(b.W, b.lo, b.n_time, b.u, b.M, b.q, b.chi, fx.ymin) for k, b in banks.items()}
+        ctx.poll(ctx.submit(ids["big"], seg["d_H"][0], seg["d_L"][0], seg["sig2_H"], seg["sig2_L"], 0),
+                 banks["big"].u.size)
+        h = ctx.submit(ids["small"], seg["d_H"][1], seg["d_L"][1], seg["sig2_H"], seg["sig2_L"], 1)
+        assert ctx.poll(h, banks["small"].u.size, timeout_us=300000) is None
+        assert ctx.serve_stats()["workers_closed"] == 0
+        assert ctx.poll(h, banks["small"].u.size) is not None
+        st = ctx.serve_stats()
+        assert st["workers_closed"] == 1 and st["workers_opened"] == 2
+        with pytest.raises(ValueError):
+            ctx.serve_set_min_idle(-1.0)
+    finally:
+        ctx.serve_stop()
