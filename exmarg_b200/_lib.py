@@ -18,8 +18,8 @@ DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 QUAD_GL64 = 16   # OR'ed into the prior: 64-point Gauss-Legendre distance quadrature
 # the plane gather's launch shapes, in exm_autotune / exm_set_gather_cfg order (warps per block x taps
-# per register group, then "pf2" where two register groups of descriptors are loaded ahead)
-GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1", "20w x1 pf2", "16w x2 pf2", "24w x1 pf2", "16w x1 pf2")
+# per register group)
+GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1")
 
 # every symbol include/exmarg_b200.h declares
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_set_filter_precision", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",

@@ -325,43 +325,40 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         lane_merge(c, t[u], vB[u], vE[u] + lwv[u], wt[u], cT, cB, cE, cS, fT, fB, fE, fS);
 }
 
-template <bool BND, int GRP, int PD, typename TE>
+template <bool BND, int GRP, typename TE>
 __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int end, unsigned &n_slow)
 {
     // the warp's sorted positions [beg, end), walked in whole chunks of EXM_DCH (positions outside
-    // [beg, end) masked); lane l takes the chunk's positions l*TPL + i, stored at i*32 + l.  The lane's
-    // register groups of GRP descriptors are numbered G = chunk * NG + g; PD groups are loaded ahead of
-    // the one in use.
-    constexpr int NG = TPL / GRP;
+    // [beg, end) masked); lane l takes the chunk's positions l*TPL + i, stored at i*32 + l
     const int lane = threadIdx.x & 31;
     const int jstart = beg & ~(EXM_DCH - 1);
-    auto load_group = [&](int G, uint4 *dst) {
-        const int jc = jstart + (G / NG) * EXM_DCH, gn = (G % NG) * GRP;
+    uint4 qa[GRP];
 #pragma unroll
-        for (int u = 0; u < GRP; ++u) {
-            const int jl = jc + TPL * lane + gn + u;
-            dst[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jc + 32 * (gn + u) + lane) : make_uint4(0u, 0u, 0u, 0u);
-        }
-    };
-    uint4 qa[PD][GRP];
-#pragma unroll
-    for (int d = 0; d < PD; ++d) load_group(d, qa[d]);
-    int G = 0;
+    for (int u = 0; u < GRP; ++u) {
+        const int jl = jstart + TPL * lane + u;
+        qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jstart + 32 * u + lane) : make_uint4(0u, 0u, 0u, 0u);
+    }
     for (int j0 = jstart; j0 < end; j0 += EXM_DCH) {
         const int jb = j0 + TPL * lane;
         int cT = -1, fT = -1;
         float cB = -1e30f, cE = 0.f, cS = 0.f, fB = -1e30f, fE = 0.f, fS = 0.f;
 #pragma unroll(kGroupUnroll)
-        for (int g = 0; g < NG; ++g, ++G) {
+        for (int g = 0; g < TPL / GRP; ++g) {
             uint4 cur[GRP];
 #pragma unroll
-            for (int u = 0; u < GRP; ++u) cur[u] = qa[0][u];
+            for (int u = 0; u < GRP; ++u) cur[u] = qa[u];
+            // the next group of descriptors (this lane's next group, or the next chunk's first)
+            const bool same = g + 1 < TPL / GRP;
+            const int jn0 = same ? j0 : j0 + EXM_DCH;
+            const int gn = same ? (g + 1) * GRP : 0;
+            if (same || j0 + EXM_DCH < end) {
 #pragma unroll
-            for (int d = 0; d + 1 < PD; ++d)
-#pragma unroll
-                for (int u = 0; u < GRP; ++u) qa[d][u] = qa[d + 1][u];
-            // group G + PD (this lane's, in this chunk or a later one; nothing past the run's end)
-            if (jstart + ((G + PD) / NG) * EXM_DCH < end) load_group(G + PD, qa[PD - 1]);
+                for (int u = 0; u < GRP; ++u) {
+                    const int jl = jn0 + TPL * lane + gn + u;
+                    qa[u] = (jl >= beg && jl < end) ? __ldg(c.descr + jn0 + 32 * (gn + u) + lane)
+                                                    : make_uint4(0u, 0u, 0u, 0u);
+                }
+            }
             tap_group<BND, GRP, TE>(a, c, cur, jb + g * GRP, j0 + 32 * g * GRP + lane, beg, end, cT, cB, cE, cS, fT,
                                     fB, fE, fS, n_slow);
         }
@@ -429,7 +426,7 @@ __device__ __forceinline__ void fold_edges(float *edge, int nw, float *aB, float
 }
 
 // this warp's equal share [w0, w1) of the run [beg, end), with its edge templates and slots
-template <bool BND, int GRP, int PD, int NW, typename TE>
+template <bool BND, int GRP, int NW, typename TE>
 __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, unsigned edge, int pair,
                                            unsigned &n_slow)
 {
@@ -468,7 +465,7 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     c.tL = tL;
     c.eF = eo;
     c.eL = eo + 16u;
-    if (w0 < w1) process_run<BND, GRP, PD, TE>(a, c, w0, w1, n_slow);
+    if (w0 < w1) process_run<BND, GRP, TE>(a, c, w0, w1, n_slow);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
@@ -483,7 +480,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 // only after pair p is done everywhere).  So at most two consecutive pairs are in flight, and the
 // consumers' accumulators alternate with the pair's parity (two warps in different pairs never
 // share a word), while the producer folds edges into a third set of its own.
-template <int NW, int GRP, int PD, typename TE>
+template <int NW, int GRP, typename TE>
 __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_constant__ CUtensorMap tmap,
                                                                 const __grid_constant__ PlaneArgs a)
 {
@@ -679,12 +676,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
                 rc.s1 = ((p + 1) % 3) * SLOT_B;
                 const int *offp = offr + p * (a.nmc + 1) + base_i;
                 rc.acc = acc_o + 4u * (3u * (p & 1) * tch);
-                warp_share<false, GRP, PD, NC, TE>(a, rc, offp[0], offp[n], edge_off(p & 1, 0), p, n_slow);
+                warp_share<false, GRP, NC, TE>(a, rc, offp[0], offp[n], edge_off(p & 1, 0), p, n_slow);
                 if (blo < bhi) {
                     rc.acc = acc_o + 4u * ((9u + 3u * (p & 1)) * tch);
                     const int bb = offp[blo], be = offp[bhi];
                     n_bnd += (lane == 0 && warp == 0) ? (unsigned)(be - bb) : 0u;
-                    warp_share<true, GRP, PD, NC, TE>(a, rc, bb, be, edge_off(p & 1, 1), p, n_slow);
+                    warp_share<true, GRP, NC, TE>(a, rc, bb, be, edge_off(p & 1, 1), p, n_slow);
                 }
             } else if (lane == 0) {   // no work: empty edge slots for the producer
                 for (int b2 = 0; b2 < 2; ++b2) {
@@ -724,35 +721,29 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     }
 }
 
-// launch shapes the autotuner chooses from: (warps per block, taps per register group, register groups of
-// descriptors loaded ahead)
+// launch shapes the autotuner chooses from: (warps per block, taps per register group)
 struct GatherCfg {
-    int nw, grp, pd;
+    int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{20, 2, 1}, {16, 2, 1}, {24, 2, 1}, {24, 1, 1},
-                                        {20, 1, 2}, {16, 2, 2}, {24, 1, 2}, {16, 1, 2}};   // warps incl. producer
+static const GatherCfg kGatherCfgs[] = {{20, 2}, {16, 2}, {24, 2}, {24, 1}};   // warps incl. producer
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
-template <int NW, int GRP0, int PD, typename TE>
+template <int NW, int GRP0, typename TE>
 static void launch_planes(exm_ctx *ctx, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     constexpr int GRP = GRP0 < TPL ? GRP0 : TPL;   // a register group never exceeds a lane's taps
-    exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP, PD, TE>, smem);
-    k_gather_planes<NW, GRP, PD, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
+    exm_allow_smem(ctx, (const void *)k_gather_planes<NW, GRP, TE>, smem);
+    k_gather_planes<NW, GRP, TE><<<grid, NW * 32, smem, ctx->stream>>>(ctx->tmap, a);
 }
 
 template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<20, 2, 1, TE>(ctx, a, grid, smem); break;
-    case 1: launch_planes<16, 2, 1, TE>(ctx, a, grid, smem); break;
-    case 2: launch_planes<24, 2, 1, TE>(ctx, a, grid, smem); break;
-    case 3: launch_planes<24, 1, 1, TE>(ctx, a, grid, smem); break;
-    case 4: launch_planes<20, 1, 2, TE>(ctx, a, grid, smem); break;
-    case 5: launch_planes<16, 2, 2, TE>(ctx, a, grid, smem); break;
-    case 6: launch_planes<24, 1, 2, TE>(ctx, a, grid, smem); break;
-    default: launch_planes<16, 1, 2, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<20, 2, TE>(ctx, a, grid, smem); break;
+    case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
+    case 2: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
+    default: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
     }
 }
 

@@ -258,11 +258,10 @@ EXM_API int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const d
  * context (same n_loud, n_random) once per shape, times each with CUDA events (reps
  * launches), keeps the fastest for later calls and writes its index to best_cfg and the
  * ms per launch of every shape to ms_per_cfg (if not NULL; room for 16 entries: this build
- * has 8 shapes, warps per block including the producer warp x taps per register group x
- * register groups of tap descriptors loaded ahead: 20x2x1, 16x2x1, 24x2x1, 24x1x1, 20x1x2,
- * 16x2x2, 24x1x2, 16x1x2).  Then, with the best shape, it times the templates per gather
+ * has 4 shapes, warps per block including the producer warp x taps per register group:
+ * 20x2, 16x2, 24x2, 24x1).  Then, with the best shape, it times the templates per gather
  * block at 50, 150 and 200 percent of the default (one wave of blocks per lag) into
- * ms_per_cfg[8..10], and keeps the best percentage (best_chunk_pct, if not NULL).
+ * ms_per_cfg[4..6], and keeps the best percentage (best_chunk_pct, if not NULL).
  * No reference counterpart (the reference takes block as a kwarg, pe.py:289-290). */
 EXM_API int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, int *best_chunk_pct,
                          double *ms_per_cfg);
