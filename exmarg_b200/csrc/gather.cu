@@ -435,8 +435,8 @@ __device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int be
     // The warps with work are a prefix: the edge fold merges equal templates of neighbouring lanes
     // only, so an empty warp between two that share a template would let both update its
     // accumulator at once.  When every warp has a chunk, the rem warps that take one more are a
-    // cyclic window that moves by rem with the pair: the same warps taking the extra chunk at every
-    // pair would leave the others waiting at every pair (a warp runs at most one pair ahead).
+    // cyclic window that moves by rem with the pair, so that no warp takes the extra chunk at every
+    // pair (measured neutral: the warps that finish a pair early leave their issue slots to the others).
     const int cb = beg / EXM_DCH, nc = (end + EXM_DCH - 1) / EXM_DCH - cb;
     const int q = nc / NW, rem = nc % NW;
     const int s = q > 0 ? (pair * rem) % NW : 0, se = s + rem;
