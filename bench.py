@@ -158,9 +158,9 @@ def measured_peaks():
 # read per node-tap both do), so the full launch's traffic is this figure times its node-taps.  The capture
 # holds only for the kernel sources it was taken on: if they changed since, traffic is reported as null.
 GATHER_TRAFFIC = {
-    "dram_bytes_per_node_tap": 3.9162,       # (1.8548e9 + 6.56e6) B / 4.7531e8 node-taps
-    "l2_read_hit_rate": 74.76,             # lts__t_sector_op_read_hit_rate.pct
-    "sources_sha256": "4c82d786e83b07ebf753fc1e6c307772303e922a79a6a8cc46ee6d9ed4172f99",
+    "dram_bytes_per_node_tap": 3.8578,       # (1.8267e9 + 6.96e6) B / 4.7531e8 node-taps
+    "l2_read_hit_rate": 75.36,             # lts__t_sector_op_read_hit_rate.pct
+    "sources_sha256": "e72dbf1d7d6c1f2bc9fe2625863df7b9bd0ff4b0f87211470e766cf915a5db0d",
     "capture": "profiles/k_gather_planes_small.md",
 }
 GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh")
