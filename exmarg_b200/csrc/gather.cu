@@ -32,7 +32,6 @@ template <typename TE> __host__ __device__ constexpr unsigned slot_bytes() { ret
 static_assert(slot_bytes<float>() % 128 == 0 && slot_bytes<__half>() % 128 == 0, "slots keep 128-byte alignment");
 #define EXM_WAIT_CYCLES (2000000000LL)   // about one second at 1.9 GHz
 #define EXM_TEST_WAIT_CYCLES (20000LL)   // the wait-expiry test's limit (no copy is ever in flight then)
-#define EXM_NOT_BND (-2147483647 - 1)   // window-row shift of a template whose boundary is at another node
 
 struct PlaneArgs {
     const uint4 *desc;
@@ -176,8 +175,8 @@ struct RunCtx {
     float sc;                   // the node's scale (16-bit tables)
     unsigned acc, accst;        // accumulator set of the run's templates (B at acc + 4 (t - lo); E, S at
                                 // + accst, + 2 accst)
-    unsigned bsh, bcf;          // boundary runs: per-template window-row shift (int; EXM_NOT_BND for a template
-                                // whose boundary is at another node) and beta fraction
+    unsigned bsh, bcf;          // boundary runs: per-template window-row shift (int) and beta fraction
+    const int *bnode;           // boundary runs: which templates have their boundary here
     int lo, m_base, n, k, r;
     int sh;                     // window row of a tap = rb0 + carry + sh (regular runs)
     int up, edge;               // fast path: row <= up, and not (row == edge with beta at the clamp)
@@ -267,14 +266,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
             atomicOr(a.err, EXM_DEVERR_BOUNDS);
             tt = -1;
         }
-        int bs = 0;   // boundary runs: the template's window-row shift, EXM_NOT_BND if its boundary is elsewhere
-        if (BND) {
-            bs = tt >= 0 ? ((const int *)gsm_f(c.bsh))[tt] : 0;
-            if (bs == EXM_NOT_BND) {
-                tt = -1;
-                bs = 0;
-            }
-        }
+        if (BND && tt >= 0 && c.bnode[tt + c.lo] != c.k) tt = -1;
         t[u] = tt;
         const int ts = tt >= 0 ? tt : 0;
         const float fb = __uint_as_float(q[u].x);
@@ -286,7 +278,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         const float sfr = fb + (BND ? gsm_f(c.bcf)[ts] : c.ckf);
         const int cy = sfr >= 1.f;
         fbf[u] = cy ? sfr - 1.f : sfr;
-        const int rb = rb0 + cy + (BND ? bs : c.sh);   // this node's window row
+        const int rb = rb0 + cy + (BND ? ((const int *)gsm_f(c.bsh))[ts] : c.sh);   // this node's window row
         constexpr int WD = TabElem<TE>::wd;
         fast[u] = (unsigned)rb <= (unsigned)c.up && rd <= WD - 2 && !(rb == c.edge && fbf[u] > 0.999999f);
         o[u] = fast[u] ? rb * WD + rd : 0;
@@ -384,10 +376,10 @@ __device__ void process_run(const PlaneArgs &a, const RunCtx &c, int beg, int en
     }
 }
 
-// the template of the lag's descriptor at sorted position j, relative to the block's first template lo
-__device__ __forceinline__ int desc_template(const uint4 *descr, int j, int m_base, int lo)
+// the template of the descriptor at sorted position j (block-local), or -1
+__device__ __forceinline__ int desc_template(const RunCtx &c, int j)
 {
-    return (int)(__ldg(&descr[exm_desc_phys(j)].w) >> 19) + m_base - lo;
+    return (int)(__ldg(&c.descr[exm_desc_phys(j)].w) >> 19) + c.m_base - c.lo;
 }
 
 // fold the warps' edge partials into the accumulators: one warp, lane w holding warp w's first (F)
@@ -433,30 +425,31 @@ __device__ __forceinline__ void fold_edges(float *edge, int nw, float *aB, float
     }
 }
 
-// the chunks of the run [beg, end) that warp `warp` of NW takes at pair `pair`: whole storage chunks, as evenly
-// as they divide (the first and last may be partial).  The warps with work are a prefix: the edge fold merges
-// equal templates of neighbouring lanes only, so an empty warp between two that share a template would let both
-// update its accumulator at once.  When every warp has a chunk, the rem warps that take one more are a cyclic
-// window that moves by rem with the pair, so that no warp takes the extra chunk at every pair.
-__device__ __forceinline__ int2 share_range(int beg, int end, int warp, int nw, int pair)
-{
-    const int cb = beg / EXM_DCH, nc = (end + EXM_DCH - 1) / EXM_DCH - cb;
-    const int q = nc / nw, rem = nc % nw;
-    const int s = q > 0 ? (pair * rem) % nw : 0, se = s + rem;
-    const int before = max(0, min(warp, se) - s) + max(0, min(warp, se - nw));   // extra chunks of warps < warp
-    const int c0 = cb + warp * q + before, c1 = c0 + q + ((warp - s + nw) % nw < rem ? 1 : 0);
-    return make_int2(max(beg, c0 * EXM_DCH), min(end, c1 * EXM_DCH));
-}
-
-// this warp's share (w0, w1, tF, tL) of a run, as the producer placed it in the share table: the positions
-// [w0, w1) and the templates of its first and last descriptors (-1 when it has none); then its edge slots
-template <bool BND, int GRP, typename TE>
-__device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int4 sh, unsigned edge, unsigned &n_slow)
+// this warp's equal share [w0, w1) of the run [beg, end), with its edge templates and slots
+template <bool BND, int GRP, int NW, typename TE>
+__device__ __forceinline__ void warp_share(const PlaneArgs &a, RunCtx &c, int beg, int end, unsigned edge, int pair,
+                                           unsigned &n_slow)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w0 = sh.x, w1 = sh.y, tF = sh.z, tL = sh.w;
+    // whole storage chunks per warp, as evenly as they divide (the first and last may be partial).
+    // The warps with work are a prefix: the edge fold merges equal templates of neighbouring lanes
+    // only, so an empty warp between two that share a template would let both update its
+    // accumulator at once.  When every warp has a chunk, the rem warps that take one more are a
+    // cyclic window that moves by rem with the pair, so that no warp takes the extra chunk at every
+    // pair: a warp runs at most one pair ahead, so with a fixed prefix the others would wait at every pair.
+    const int cb = beg / EXM_DCH, nc = (end + EXM_DCH - 1) / EXM_DCH - cb;
+    const int q = nc / NW, rem = nc % NW;
+    const int s = q > 0 ? (pair * rem) % NW : 0, se = s + rem;
+    const int before = max(0, min(warp, se) - s) + max(0, min(warp, se - NW));   // extra chunks of warps < warp
+    const int c0 = cb + warp * q + before, c1 = c0 + q + ((warp - s + NW) % NW < rem ? 1 : 0);
+    const int w0 = max(beg, c0 * EXM_DCH), w1 = min(end, c1 * EXM_DCH);
     const unsigned eo = edge + 32u * warp;   // 8 floats per warp
     float *e = gsm_f(eo);
+    int tF = -1, tL = -1;
+    if (w0 < w1) {
+        tF = desc_template(c, w0);
+        tL = desc_template(c, w1 - 1);
+    }
     if (lane == 0) {
         e[0] = -1e30f;
         e[1] = 0.f;
@@ -512,8 +505,6 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     const unsigned qcnt_o = edge_o + 4u * (2 * 2 * 8 * 32), qent_o = qcnt_o + 4u * 3 * 32;
     int *qcnt = (int *)(smem + qcnt_o);
     const int2 *qent = (const int2 *)(smem + qent_o);
-    // share table [pair mod 3][regular, boundary run][consumer warp]: (w0, w1, tF, tL), written by the producer
-    int4 *shr = (int4 *)(smem + qent_o + 8u * 3 * 32 * EXM_SLOWQ);
     auto edge_off = [&](int par, int b2) { return edge_o + 4u * (unsigned)((par * 2 + b2) * 8 * NC); };
     __shared__ int bl_sh[2];
     __shared__ unsigned bad_sh;
@@ -553,8 +544,6 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             bcf[j] = (float)(cbv - f);
             atomicMin(&bl_sh[0], j);
             atomicMax(&bl_sh[1], j + 1);
-        } else {
-            bsh[j] = EXM_NOT_BND;
         }
     }
     if (tid == 0) {
@@ -565,39 +554,15 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
     __syncthreads();
     const int blo = bl_sh[0], bhi = bl_sh[1];
     unsigned n_slow = 0, n_bnd = 0;
-    const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);   // run starts per (pair, template)
-    const int base_i = lo - a.m_base;                                    // chunk-local index of template lo
 
     if (warp == NC) {
         // ---------------------------------------------------------------- producer
         const int32_t *tsr_all = a.tside + (long long)rl * a.per_lag;
-        const uint4 *dl = a.desc + (long long)rl * a.per_lag;
-        // the consumers' shares of pair q's regular and boundary runs into slot q % 3 of the share table, lane w
-        // for warp w.  The consumers read them once planes q and q + 1 are staged: the arrive that precedes
-        // the copy of plane q + 1 releases them (its slot held pair q - 3's shares, read before pair q - 2 was
-        // done everywhere).
-        auto put_shares = [&](int q) {
-            if (q >= EXM_NPAIR) return;
-            const int *offq = offr + q * (a.nmc + 1) + base_i;
-            int4 *tb = shr + (q % 3) * 64;
-            for (int pass = 0; pass < (blo < bhi ? 2 : 1); ++pass) {
-                const int beg = pass ? offq[blo] : offq[0], end = pass ? offq[bhi] : offq[n];
-                if (lane == 0 && pass == 1) n_bnd += (unsigned)(end - beg);
-                if (lane < NC) {
-                    const int2 w = share_range(beg, end, lane, NC, q);
-                    const int tF = w.x < w.y ? desc_template(dl, w.x, a.m_base, lo) : -1;
-                    const int tL = w.x < w.y ? desc_template(dl, w.y - 1, a.m_base, lo) : -1;
-                    tb[pass * 32 + lane] = make_int4(w.x, w.y, tF, tL);
-                }
-            }
-            __syncwarp();
-        };
         int issued = 0;
         if (a.stage) {
-            for (int q = 0; q < 3 && q < a.nphif; ++q) {
-                if (q >= 1) put_shares(q - 1);
-                if (lane == 0) tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
-            }
+            if (lane == 0)
+                for (int q = 0; q < 3 && q < a.nphif; ++q)
+                    tma_load_plane(&tmap, &full[q], win + q * SLOT, C0, R0, q, r, k, SLOT_B);
             issued = min(3, a.nphif);
         }
         bool ok = true;
@@ -608,9 +573,8 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             if (blo < bhi)
                 fold_edges(gsm_f(edge_off(p & 1, 1)), NC, acc + 15 * tch, acc + 16 * tch, acc + 17 * tch, n);
             __syncwarp();
-            // plane p is no longer needed anywhere: its slot takes plane p + 3, after pair p + 2's shares
+            // plane p is no longer needed anywhere: its slot takes plane p + 3
             if (a.stage && p + 3 < a.nphif) {
-                put_shares(p + 2);
                 if (lane == 0) tma_load_plane(&tmap, &full[p % 3], win + (p % 3) * SLOT, C0, R0, p + 3, r, k, SLOT_B);
                 ++issued;
             }
@@ -677,12 +641,14 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         }
     } else {
         // ---------------------------------------------------------------- consumers
+        const int *offr = a.off + (long long)rl * EXM_NPAIR * (a.nmc + 1);
         RunCtx rc;
         rc.descr = a.desc + (long long)rl * a.per_lag;
         rc.tsr = a.tside + (long long)rl * a.per_lag;
         rc.bsh = bsh_o;
         rc.bcf = bcf_o;
         rc.accst = 4u * tch;
+        rc.bnode = a.bnode;
         rc.lo = lo;
         rc.m_base = a.m_base;
         rc.n = n;
@@ -694,6 +660,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         rc.k = k;
         rc.r = r;
         rc.lw = a.lw;
+        const int base_i = lo - a.m_base;   // chunk-local index of template lo
         bool ok = true;
         for (int p = 0; p < EXM_NPAIR; ++p) {
             // warp-uniform: the lanes go on to shuffles together
@@ -707,12 +674,14 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             if (ok) {
                 rc.s0 = (p % 3) * SLOT_B;
                 rc.s1 = ((p + 1) % 3) * SLOT_B;
-                const int4 *tb = shr + (p % 3) * 64;
+                const int *offp = offr + p * (a.nmc + 1) + base_i;
                 rc.acc = acc_o + 4u * (3u * (p & 1) * tch);
-                warp_share<false, GRP, TE>(a, rc, tb[warp], edge_off(p & 1, 0), n_slow);
+                warp_share<false, GRP, NC, TE>(a, rc, offp[0], offp[n], edge_off(p & 1, 0), p, n_slow);
                 if (blo < bhi) {
                     rc.acc = acc_o + 4u * ((9u + 3u * (p & 1)) * tch);
-                    warp_share<true, GRP, TE>(a, rc, tb[32 + warp], edge_off(p & 1, 1), n_slow);
+                    const int bb = offp[blo], be = offp[bhi];
+                    n_bnd += (lane == 0 && warp == 0) ? (unsigned)(be - bb) : 0u;
+                    warp_share<true, GRP, NC, TE>(a, rc, bb, be, edge_off(p & 1, 1), p, n_slow);
                 }
             } else if (lane == 0) {   // no work: empty edge slots for the producer
                 for (int b2 = 0; b2 < 2; ++b2) {
@@ -793,17 +762,15 @@ int exm_gather_num_cfgs() { return kNumGatherCfgs; }
 static size_t planes_smem(int tch, int dtype)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(dtype) * exm_dtype_bytes(dtype);
-    // 6 accumulator sets of 3 floats, bcf, bsh; edge slots; exact-path queue counts and entries; share table
-    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 +
-           3 * 64 * 16;
+    // 6 accumulator sets of 3 floats, bcf, bsh; edge slots; exact-path queue counts and entries
+    return 3 * slot + 64 + (size_t)tch * 20 * 4 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8;
 }
 
 // the most templates a block can hold in shared memory next to the staged planes
 static int planes_tch_max(exm_ctx *ctx)
 {
     const size_t slot = (size_t)EXM_WB * exm_dtype_wd(ctx->dtype) * exm_dtype_bytes(ctx->dtype);
-    const size_t fixed =
-        3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 3 * 64 * 16 + 2048;   // + static
+    const size_t fixed = 3 * slot + 64 + 2 * 2 * 8 * 32 * 4 + 3 * 32 * 4 + 3 * 32 * EXM_SLOWQ * 8 + 2048;   // + static
     const size_t room = ctx->smem_optin > fixed ? ctx->smem_optin - fixed : 0;
     return (int)std::min<size_t>(EXM_TCH, room / (20 * 4) / 16 * 16);
 }
