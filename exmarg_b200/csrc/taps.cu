@@ -188,10 +188,15 @@ __global__ void __launch_bounds__(1024) k_tap_scan(int *cnt, int nmc)
 }
 
 // descriptors, stably scattered to their (lag, pair, template) runs: one block per template,
-// every lag of the chunk in turn
+// every lag of the chunk in turn.  A batch is SCATTER_ROUNDS rounds of 256 walked times (k = k0 + m 256 +
+// thread): each warp counts its taps per pair in each round, 48 threads turn the counts into exclusive
+// prefixes in (round, warp) order -- the order of k -- and every tap lands at its run's base + the prefix + its
+// rank among equal pairs in the warp: the same positions as one walked time per thread and round, with four
+// block barriers per batch instead of four per round.
+#define SCATTER_ROUNDS 4
 __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
 {
-    __shared__ int wcnt[8][EXM_NPAIR];
+    __shared__ int wcnt[SCATTER_ROUNDS][8][EXM_NPAIR];
     __shared__ int base[EXM_NPAIR];
     extern __shared__ unsigned char wsm[];
     const int i = blockIdx.x;
@@ -215,49 +220,60 @@ __global__ void __launch_bounds__(256) k_tap_scatter(TapArgs a, int rc)
         int32_t *tside = a.tside + (long long)rl * a.pitch;
         __syncthreads();
         for (int q = threadIdx.x; q < EXM_NPAIR; q += blockDim.x) base[q] = off[q * (a.nmc + 1) + i];
-        for (int k0 = 0; k0 < a.nwalk; k0 += blockDim.x) {
-            for (int q = threadIdx.x; q < 8 * EXM_NPAIR; q += blockDim.x) (&wcnt[0][0])[q] = 0;
+        for (int k0 = 0; k0 < a.nwalk; k0 += SCATTER_ROUNDS * 256) {
+            for (int q = threadIdx.x; q < SCATTER_ROUNDS * 8 * EXM_NPAIR; q += blockDim.x) (&wcnt[0][0][0])[q] = 0;
             __syncthreads();
-            const int k = k0 + threadIdx.x;
-            int p = -1, t = 0, flag = 0, ib = 0, d0 = 0;
-            float w = 0.f, fb = 0.f, fd = 0.f;
-            if (k < a.nwalk) {
-                float2 l;
-                float llo;
-                walk_at(a, i, L, Llo, wc, k, t, flag, l, llo);
-                int i1 = t + tau0;
-                if (i1 >= nt) i1 -= nt;
-                exm_tap_geom(l, H[i1], llo, Hlo ? Hlo[i1] : 0.f, boff, a.g, p, w, ib, fb, d0, fd);
-            }
-            const unsigned peers = __match_any_sync(0xffffffffu, p);
-            const int rk = __popc(peers & lt);
-            if (p >= 0 && rk == 0) wcnt[warp][p] = __popc(peers);
-            __syncthreads();
-            int pos = 0;
-            if (p >= 0) {
-                int pre = 0;
-                for (int ww = 0; ww < warp; ++ww) pre += wcnt[ww][p];
-                pos = base[p] + pre + rk;
-            }
-            __syncthreads();
-            if (threadIdx.x < EXM_NPAIR) {
-                int s2 = 0;
-                for (int ww = 0; ww < 8; ++ww) s2 += wcnt[ww][threadIdx.x];
-                base[threadIdx.x] += s2;
-            }
-            if (p >= 0 && pos >= 0 && pos < a.per_lag) {
-                uint4 d;
-                d.x = __float_as_uint(fb);
-                d.y = __float_as_uint(fd);
-                d.z = __float_as_uint(w) | ((unsigned)flag << 31);
+            int p[SCATTER_ROUNDS], rk[SCATTER_ROUNDS], tt[SCATTER_ROUNDS];
+            uint4 d[SCATTER_ROUNDS];
+#pragma unroll
+            for (int m = 0; m < SCATTER_ROUNDS; ++m) {
+                const int k = k0 + m * 256 + threadIdx.x;
+                int t = 0, flag = 0, ib = 0, d0 = 0;
+                float w = 0.f, fb = 0.f, fd = 0.f;
+                p[m] = -1;
+                if (k < a.nwalk) {
+                    float2 l;
+                    float llo;
+                    walk_at(a, i, L, Llo, wc, k, t, flag, l, llo);
+                    int i1 = t + tau0;
+                    if (i1 >= nt) i1 -= nt;
+                    exm_tap_geom(l, H[i1], llo, Hlo ? Hlo[i1] : 0.f, boff, a.g, p[m], w, ib, fb, d0, fd);
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, p[m]);
+                rk[m] = __popc(peers & lt);
+                if (p[m] >= 0 && rk[m] == 0) wcnt[m][warp][p[m]] = __popc(peers);
+                d[m].x = __float_as_uint(fb);
+                d[m].y = __float_as_uint(fd);
+                d[m].z = __float_as_uint(w) | ((unsigned)flag << 31);
                 int rd = d0 - C0, rb0 = ib - Rh;
                 if ((unsigned)rd > (unsigned)(a.wd - 2) || rb0 < -1024 || rb0 > 1023) {
                     rd = 255;   // outside every node's window: the exact path
                     rb0 = 0;
                 }
-                d.w = ((unsigned)i << 19) | ((unsigned)rd << 11) | ((unsigned)rb0 & 0x7FFu);
-                desc[pos] = d;   // sorted order; k_tap_interleave rearranges each chunk afterwards
-                tside[pos] = t;
+                d[m].w = ((unsigned)i << 19) | ((unsigned)rd << 11) | ((unsigned)rb0 & 0x7FFu);
+                tt[m] = t;
+            }
+            __syncthreads();
+            if (threadIdx.x < EXM_NPAIR) {   // exclusive prefixes per pair in (round, warp) order, from the run base
+                const int q = threadIdx.x;
+                int run = base[q];
+                for (int m = 0; m < SCATTER_ROUNDS; ++m)
+                    for (int ww = 0; ww < 8; ++ww) {
+                        const int v = wcnt[m][ww][q];
+                        wcnt[m][ww][q] = run;
+                        run += v;
+                    }
+                base[q] = run;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < SCATTER_ROUNDS; ++m) {
+                if (p[m] < 0) continue;
+                const int pos = wcnt[m][warp][p[m]] + rk[m];
+                if (pos >= 0 && pos < a.per_lag) {
+                    desc[pos] = d[m];   // sorted order; k_tap_interleave rearranges each chunk afterwards
+                    tside[pos] = tt[m];
+                }
             }
             __syncthreads();
         }
