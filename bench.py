@@ -158,9 +158,9 @@ def measured_peaks():
 # read per node-tap both do), so the full launch's traffic is this figure times its node-taps.  The capture
 # holds only for the kernel sources it was taken on: if they changed since, traffic is reported as null.
 GATHER_TRAFFIC = {
-    "dram_bytes_per_node_tap": 3.7434,       # (1.7693e9 + 9.98e6) B / 4.7531e8 node-taps
-    "l2_read_hit_rate": 75.73,             # lts__t_sector_op_read_hit_rate.pct
-    "sources_sha256": "f3cc0f6ba9012b69662a73526738665f2ce1213c22b3ee1f212853f53606400f",
+    "dram_bytes_per_node_tap": 3.7256,       # (1.761e9 + 9.57e6) B / 4.7531e8 node-taps
+    "l2_read_hit_rate": 76.07,             # lts__t_sector_op_read_hit_rate.pct
+    "sources_sha256": "eb531ba4a75ac286697b1ea48c4a20a1b41472f24f84626550d228795bbe8698",
     "capture": "profiles/k_gather_planes_small.md",
 }
 GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh")
