@@ -158,9 +158,9 @@ def measured_peaks():
 # read per node-tap both do), so the full launch's traffic is this figure times its node-taps.  The capture
 # holds only for the kernel sources it was taken on: if they changed since, traffic is reported as null.
 GATHER_TRAFFIC = {
-    "dram_bytes_per_node_tap": 3.7256,       # (1.761e9 + 9.57e6) B / 4.7531e8 node-taps
-    "l2_read_hit_rate": 76.07,             # lts__t_sector_op_read_hit_rate.pct
-    "sources_sha256": "eb531ba4a75ac286697b1ea48c4a20a1b41472f24f84626550d228795bbe8698",
+    "dram_bytes_per_node_tap": 3.9683,       # (1.8772e9 + 8.92e6) B / 4.7531e8 node-taps (28 warps x 1, 150 %)
+    "l2_read_hit_rate": 69.92,             # lts__t_sector_op_read_hit_rate.pct
+    "sources_sha256": "6014a92f6f6972047daeb8f5535a10d004f69fd2b89c0258d722db9f213bc2f9",
     "capture": "profiles/k_gather_planes_small.md",
 }
 GATHER_SOURCES = ("exmarg_b200/csrc/gather.cu", "exmarg_b200/csrc/taps.cu", "exmarg_b200/csrc/kernels.cuh")

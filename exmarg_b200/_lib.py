@@ -19,7 +19,7 @@ PRIOR_VOLUME, PRIOR_TABULATED = 0, 1
 QUAD_GL64 = 16   # OR'ed into the prior: 64-point Gauss-Legendre distance quadrature
 # the plane gather's launch shapes, in exm_autotune / exm_set_gather_cfg order (warps per block x taps
 # per register group)
-GATHER_SHAPES = ("20w x2", "16w x2", "24w x2", "24w x1")
+GATHER_SHAPES = ("28w x1", "16w x2", "24w x2", "24w x1", "20w x2")
 
 # every symbol include/exmarg_b200.h declares
 SYMBOLS = ("exm_version", "exm_rng_integers", "exm_gauss_legendre", "exm_device_memory", "exm_ctx_timing", "exm_ctx_create_sharing", "exm_ctx_set_graph", "exm_ctx_set_priority", "exm_ctx_test_wait_expiry", "exm_ctx_set_filter_precision", "exm_ctx_create", "exm_ctx_destroy", "exm_last_error", "exm_ctx_bytes", "exm_store_init",
@@ -163,7 +163,7 @@ class Context:
         self.prep_token = None
         self.nm = self.nfreq = self.n_time = None
         self.gather_cfg = None          # the launch shape chosen by autotune or set_gather_cfg (None: default)
-        self.gather_chunk_pct = 100     # templates per gather block, percent of the default
+        self.gather_chunk_pct = 150     # templates per gather block, percent of one wave of blocks per lag
         self.store_shape = None         # (nodes, lags, phase planes, nb, nd, dtype) of the resident store
         self.device_total = device_memory(device)[1]   # identifies the device model in the autotune cache
 

@@ -131,7 +131,7 @@ struct exm_ctx {
     // launch shape of the plane gather (index into its table; chosen by exm_autotune)
     struct exm_redshift *rs = nullptr;   // pe_redshift's grid and buffers (csrc/redshift.cu)
     int gather_cfg = 0;
-    int gather_chunk_pct = 100;
+    int gather_chunk_pct = 150;
     bool test_wait_expiry = false;
     bool traj_fp64 = false;          // filter precision 'fp64': the ln|z| residual is kept and used by the taps
     exm_server *srv = nullptr;       // request loop served from this context (exm_serve_start)   // the plane gather stages nothing and its barrier waits run out (a test)   // templates per gather block, percent of the one-wave-per-lag size

@@ -175,8 +175,8 @@ struct RunCtx {
     float sc;                   // the node's scale (16-bit tables)
     unsigned acc, accst;        // accumulator set of the run's templates (B at acc + 4 (t - lo); E, S at
                                 // + accst, + 2 accst)
-    unsigned bsh, bcf;          // boundary runs: per-template window-row shift (int) and beta fraction
-    const int *bnode;           // boundary runs: which templates have their boundary here
+    unsigned bsh, bcf;          // boundary runs: per-template window-row shift (int; EXM_BSH_NONE for templates
+                                // whose boundary point is not this node) and beta fraction
     int lo, m_base, n, k, r;
     int sh;                     // window row of a tap = rb0 + carry + sh (regular runs)
     int up, edge;               // fast path: row <= up, and not (row == edge with beta at the clamp)
@@ -205,6 +205,7 @@ __device__ __forceinline__ void acc_merge(const RunCtx &c, int tr, float B, floa
 #endif
 constexpr int kGroupUnroll = EXM_GUNROLL;   // tap groups of a chunk unrolled in the lane loop
 #define EXM_SLOWQ 8   // exact-path taps a consumer warp queues per plane pair for the producer
+#define EXM_BSH_NONE (-(1 << 28))   // bsh entry of a template whose boundary point is another node
 
 
 // the lane-local running segmented merge of one value (taps arrive sorted by template)
@@ -266,7 +267,12 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
             atomicOr(a.err, EXM_DEVERR_BOUNDS);
             tt = -1;
         }
-        if (BND && tt >= 0 && c.bnode[tt + c.lo] != c.k) tt = -1;
+        // boundary runs: the template's window-row shift, EXM_BSH_NONE unless its boundary point is this node
+        int bs = 0;
+        if (BND) {
+            bs = tt >= 0 ? ((const int *)gsm_f(c.bsh))[tt] : EXM_BSH_NONE;
+            if (bs == EXM_BSH_NONE) tt = -1;
+        }
         t[u] = tt;
         const int ts = tt >= 0 ? tt : 0;
         const float fb = __uint_as_float(q[u].x);
@@ -278,7 +284,7 @@ __device__ __forceinline__ void tap_group(const PlaneArgs &a, const RunCtx &c, c
         const float sfr = fb + (BND ? gsm_f(c.bcf)[ts] : c.ckf);
         const int cy = sfr >= 1.f;
         fbf[u] = cy ? sfr - 1.f : sfr;
-        const int rb = rb0 + cy + (BND ? ((const int *)gsm_f(c.bsh))[ts] : c.sh);   // this node's window row
+        const int rb = rb0 + cy + (BND ? bs : c.sh);   // this node's window row
         constexpr int WD = TabElem<TE>::wd;
         fast[u] = (unsigned)rb <= (unsigned)c.up && rd <= WD - 2 && !(rb == c.edge && fbf[u] > 0.999999f);
         o[u] = fast[u] ? rb * WD + rd : 0;
@@ -537,6 +543,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
             acc[(3 * q + 1) * tch + j] = 0.f;
             acc[(3 * q + 2) * tch + j] = 0.f;
         }
+        bsh[j] = EXM_BSH_NONE;
         if (a.bnode[lo + j] == k) {
             const double cbv = a.cb[lo + j];
             const double f = floor(cbv);
@@ -648,7 +655,6 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
         rc.bsh = bsh_o;
         rc.bcf = bcf_o;
         rc.accst = 4u * tch;
-        rc.bnode = a.bnode;
         rc.lo = lo;
         rc.m_base = a.m_base;
         rc.n = n;
@@ -725,7 +731,8 @@ __global__ void __launch_bounds__(NW * 32, 1) k_gather_planes(const __grid_const
 struct GatherCfg {
     int nw, grp;
 };
-static const GatherCfg kGatherCfgs[] = {{20, 2}, {16, 2}, {24, 2}, {24, 1}};   // warps incl. producer
+// warps incl. producer x taps per register group; the first is the default of an untuned context
+static const GatherCfg kGatherCfgs[] = {{28, 1}, {16, 2}, {24, 2}, {24, 1}, {20, 2}};
 static const int kNumGatherCfgs = (int)(sizeof(kGatherCfgs) / sizeof(kGatherCfgs[0]));
 
 template <int NW, int GRP0, typename TE>
@@ -740,10 +747,11 @@ template <typename TE>
 static void launch_cfg_t(exm_ctx *ctx, int cfg, const PlaneArgs &a, dim3 grid, size_t smem)
 {
     switch (cfg) {
-    case 0: launch_planes<20, 2, TE>(ctx, a, grid, smem); break;
+    case 0: launch_planes<28, 1, TE>(ctx, a, grid, smem); break;
     case 1: launch_planes<16, 2, TE>(ctx, a, grid, smem); break;
     case 2: launch_planes<24, 2, TE>(ctx, a, grid, smem); break;
-    default: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
+    case 3: launch_planes<24, 1, TE>(ctx, a, grid, smem); break;
+    default: launch_planes<20, 2, TE>(ctx, a, grid, smem); break;
     }
 }
 

@@ -258,16 +258,18 @@ EXM_API int exm_pe_intrinsic(exm_ctx *ctx, int n_seg, const double *d_H, const d
  * context (same n_loud, n_random) once per shape, times each with CUDA events (reps
  * launches), keeps the fastest for later calls and writes its index to best_cfg and the
  * ms per launch of every shape to ms_per_cfg (if not NULL; room for 16 entries: this build
- * has 4 shapes, warps per block including the producer warp x taps per register group:
- * 20x2, 16x2, 24x2, 24x1).  Then, with the best shape, it times the templates per gather
- * block at 50, 150 and 200 percent of the default (one wave of blocks per lag) into
- * ms_per_cfg[4..6], and keeps the best percentage (best_chunk_pct, if not NULL).
+ * has 5 shapes, warps per block including the producer warp x taps per register group:
+ * 28x1 (an untuned context's), 16x2, 24x2, 24x1, 20x2).  Then, with the best shape, it times
+ * the templates per gather block at 50, 150 and 200 percent of one wave of blocks per lag
+ * (measured at 100) into ms_per_cfg[5..7], and keeps the best percentage (best_chunk_pct, if
+ * not NULL; an untuned context uses 150).
  * No reference counterpart (the reference takes block as a kwarg, pe.py:289-290). */
 EXM_API int exm_autotune(exm_ctx *ctx, int n_loud, int n_random, int reps, int *best_cfg, int *best_chunk_pct,
                          double *ms_per_cfg);
 
 /* Select a launch shape of the plane gather by index (as exm_autotune reports it) and the
- * templates per gather block in percent of the default (10..1000; 0 keeps the current). */
+ * templates per gather block in percent of one wave of blocks per lag (10..1000; 0 keeps the
+ * current; an untuned context uses shape 0 at 150). */
 EXM_API int exm_set_gather_cfg(exm_ctx *ctx, int cfg, int chunk_pct);
 
 /* ------------------------------------------------------------------ serving (native request loop) */

@@ -18,7 +18,7 @@ def _setup():
     fx = Fixture("config1")
     big = fx.b200_bank()
     ctx = eb.prepare(big, fx.store, fx.prior_arg, fx.ymin)
-    ctx.set_gather_cfg(0, 100)
+    ctx.set_gather_cfg(0, 150)
     M, q, chi = (fx.rows[:24, i] for i in range(3))
     small = MassBank(M, q, chi, fx.seg, "b200", W=fx.W[:24], u=fx.u[:24])
     seg = eb.read_segments(fx.seg)

@@ -32,7 +32,7 @@ def test_every_shape_and_chunk_matches_reference(name):
                 assert err <= TOL_LNB, (_lib.GATHER_SHAPES[cfg], pct, err)
                 assert np.abs(res["ln_lambda"] - fx.ln_lambda).max() <= 1e-4
     finally:
-        ctx.set_gather_cfg(0, 100)
+        ctx.set_gather_cfg(0, 150)
 
 
 def test_autotune_keeps_a_valid_choice():
@@ -48,7 +48,7 @@ def test_autotune_keeps_a_valid_choice():
         res = _pe(fx, bank)
         assert np.abs(res["ln_b"] - fx.ln_b).max() <= TOL_LNB
     finally:
-        bank.ctx.set_gather_cfg(0, 100)
+        bank.ctx.set_gather_cfg(0, 150)
 
 
 def test_bad_shape_is_rejected():
