@@ -427,6 +427,38 @@ extern "C" void exm_ctx_destroy(exm_ctx *ctx)
     if (free_parent) ctx_free(free_parent);
 }
 
+// the calling thread's last failure on a context (by the address of its message), and its last read
+static thread_local const exm_errmsg *tl_err_owner = nullptr;
+static thread_local std::string tl_err_msg, tl_err_read;
+
+exm_errmsg &exm_errmsg::operator=(const std::string &m)
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        msg_ = m;
+    }
+    tl_err_owner = this;
+    tl_err_msg = m;
+    return *this;
+}
+
+exm_errmsg::operator std::string() const
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    return msg_;
+}
+
+const char *exm_errmsg::c_str() const
+{
+    if (tl_err_owner == this) {
+        tl_err_read = tl_err_msg;
+    } else {
+        std::lock_guard<std::mutex> lk(mu_);
+        tl_err_read = msg_;
+    }
+    return tl_err_read.c_str();
+}
+
 extern "C" const char *exm_last_error(const exm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 extern "C" size_t exm_ctx_bytes(const exm_ctx *ctx) { return ctx ? ctx->used : 0; }

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -76,11 +77,26 @@ struct exm_slot {
 
 #define EXM_MAX_REJ 4096
 
+// The last error message of a context.  The serving entry points (exm_submit, exm_poll, ...) may fail on several
+// host threads at once, so an assignment is serialised, and a thread reading the message gets a copy that stays
+// valid until its next read: the message of its own last failed call on this context if it has one, else the
+// context's latest.  Single-threaded callers see the plain last message, as before.
+struct exm_errmsg {
+    exm_errmsg &operator=(const std::string &m);
+    exm_errmsg &operator=(const char *m) { return *this = std::string(m); }
+    operator std::string() const;   // the context's latest message (a copy)
+    const char *c_str() const;      // as described above; valid until this thread's next c_str()
+
+  private:
+    mutable std::mutex mu_;
+    std::string msg_;
+};
+
 struct exm_ctx {
     int dev = 0;
     size_t budget = 0, used = 0;
     cudaStream_t stream = nullptr;
-    std::string err;
+    exm_errmsg err;
     int sm_count = 148;
     size_t smem_optin = 0;
 

@@ -212,7 +212,7 @@ static void worker_main(exm_server *s, SrvWorker *w)
             rc = exm_pe_prepare(w->ctx, bk.ymin, bk.prior, bk.lny.empty() ? nullptr : bk.lny.data(),
                                 bk.p.empty() ? nullptr : bk.p.data(), (int)bk.lny.size());
         if (rc == EXM_OK && s->graph) rc = exm_ctx_set_graph(w->ctx, 1);
-        if (rc != EXM_OK) err = w->ctx->err;
+        if (rc != EXM_OK) err = std::string(w->ctx->err);
     }
     int greatest = 0, least = 0;
     cudaSetDevice(s->parent->dev);
@@ -237,7 +237,7 @@ static void worker_main(exm_server *s, SrvWorker *w)
             if (want != prio && exm_ctx_set_priority(w->ctx, want, nullptr) == EXM_OK) prio = want;
             rc2 = exm_pe_intrinsic(w->ctx, 1, r->dH.data(), r->dL.data(), r->s2H.data(), r->s2L.data(), &r->seed,
                                    s->n_loud, s->n_random, lnl.data(), &lnb);
-            if (rc2 != EXM_OK) msg = w->ctx->err;
+            if (rc2 != EXM_OK) msg = std::string(w->ctx->err);
             bytes = w->ctx->used;
         }
         std::vector<std::unique_ptr<SrvWorker>> closed;

@@ -78,6 +78,9 @@ EXM_API int exm_ctx_set_graph(exm_ctx *ctx, int enable);
  * segment's gather lead while the others fill its gaps, instead of interleaving all of them
  * (which multiplies the tap descriptors resident in L2).  No reference counterpart. */
 EXM_API int exm_ctx_set_priority(exm_ctx *ctx, int priority, int *range_out);
+/* The message of the last failed call on ctx.  With calls on several host threads (exm_submit and
+ * exm_poll allow it), each thread gets the message of its own last failed call on ctx (else ctx's
+ * latest); the pointer stays valid until the same thread calls exm_last_error again. */
 EXM_API const char *exm_last_error(const exm_ctx *ctx);
 
 /* Precision of the trajectories the table reads see.  EXM_FILTER_REFERENCE (the default): ln|z| and arg z

@@ -124,3 +124,53 @@ def test_minimum_idle_time_before_closing_a_worker():
             ctx.serve_set_min_idle(-1.0)
     finally:
         ctx.serve_stop()
+
+
+def test_concurrent_pollers_read_their_own_error_messages():
+    # exm_submit / exm_poll may be called from several host threads (ctypes releases the GIL, so these threads
+    # are in the library at the same time): every failed poll's message must be intact and the calling
+    # thread's own -- its handle's "has not finished", or the bogus handle it asked for
+    import ctypes
+    import threading
+    fx, ctx, banks, seg = _setup()
+    b = banks["small"]
+    ctx.serve_start(hbm_budget=0, max_workers=1, n_loud=fx.n_loud, n_random=fx.n_random)
+    lib, h = ctx.lib, ctx.h
+    bad = []
+    try:
+        bid = ctx.serve_add_bank(b.W, b.lo, b.n_time, b.u, b.M, b.q, b.chi, fx.ymin)
+        handles = [ctx.submit(bid, seg["d_H"][i % 2], seg["d_L"][i % 2], seg["sig2_H"], seg["sig2_L"], i)
+                   for i in range(6)]
+
+        def own(hd):
+            lnl = np.empty(b.u.size, np.float64)
+            lnb = ctypes.c_double()
+            while True:
+                rc = lib.exm_poll(h, int(hd), 0, lnl.ctypes.data_as(ctypes.c_void_p), ctypes.byref(lnb))
+                if rc == _lib.EXM_OK:
+                    return
+                msg = lib.exm_last_error(h).decode()
+                if rc != _lib.EXM_ERR_TIMEOUT or msg != "request %d has not finished" % hd:
+                    bad.append((hd, rc, msg))
+                    return
+
+        def bogus(k):
+            for _ in range(2000):
+                rc = lib.exm_poll(h, 10 ** 9 + k, 0, None, None)
+                msg = lib.exm_last_error(h).decode()
+                if rc != _lib.EXM_ERR_ARG or not msg.startswith("unknown request handle"):
+                    bad.append((k, rc, msg))
+                    return
+
+        threads = [threading.Thread(target=own, args=(hd,)) for hd in handles]
+        threads += [threading.Thread(target=bogus, args=(k,)) for k in range(3)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join(timeout=120)
+        assert not any(t.is_alive() for t in threads)
+        assert not bad, bad[:3]
+        st = ctx.serve_stats()
+        assert st["served"] == len(handles) and st["failed"] == 0
+    finally:
+        ctx.serve_stop()
