@@ -115,6 +115,15 @@ class Scheduler:
     def release(self, w):
         self.busy.discard(w)
 
+    def forget(self, w):
+        """drop worker w (one that could not be opened): its slot and budget are free again"""
+        self.busy.discard(w)
+        for key, ws in self.workers.items():
+            if w in ws:
+                ws.remove(w)
+                self.used -= self.cost(key)
+                return
+
     def recost(self, key, new_cost, set_cost):
         """replace key's per-worker cost (an estimate by a measured figure); set_cost(key, c) updates the
         table self.cost reads, and the budget in use follows for key's live workers"""
@@ -196,8 +205,8 @@ class Server:
 
     def _worker_for(self, wid, key):
         if wid not in self.workers:
-            self.n_created += 1
             self.workers[wid] = _Worker(self.parent, self.banks[key], self.store, self.prior, self.ymin, self.graph)
+            self.n_created += 1
         return self.workers[wid]
 
     def _run(self, req, wid):
@@ -239,7 +248,17 @@ class Server:
             if req is None:
                 return n
             if new:
-                self._worker_for(wid, key)
+                try:
+                    self._worker_for(wid, key)
+                except Exception as e:   # the worker could not open (e.g. device memory): its request fails
+                    with self.lock:
+                        self.sched.forget(wid)
+                    req.t_done = time.perf_counter()
+                    req.future.set_exception(e)
+                    with self.lock:
+                        self.done.append(req)
+                        self.lock.notify_all()
+                    continue
             t = threading.Thread(target=self._run, args=(req, wid), daemon=True)
             t.start()
             self._threads.append(t)

@@ -101,3 +101,46 @@ def test_busy_bank_waits_instead_of_evicting():
     assert g[0] is None and g[4] == []                  # no second 'a' worker at the price of 'b''s
     s.release(a[2])
     assert s.admit()[0] == "a1"
+
+
+def test_a_worker_that_cannot_open_fails_its_request_and_frees_its_budget(monkeypatch):
+    # the server's host logic with fakes for the device: bank 'bad' cannot get a worker (its context runs
+    # out of memory); its request must fail with that error instead of waiting forever, the slot and budget
+    # must come back, and the other bank's requests are served
+    from types import SimpleNamespace
+
+    import numpy as np
+    import pytest
+
+    from exmarg_b200 import serve
+
+    class FakeWorker:
+        def __init__(self, parent, bank, store, prior, ymin, graph=False):
+            if bank.name == "bad":
+                raise MemoryError("no room for the workspace")
+            self.ctx = SimpleNamespace(bytes=10)
+
+        def prioritise(self, rank):
+            pass
+
+        def run(self, segments, row, seed, n_loud, n_random):
+            return np.array([[float(seed)]]), np.array([1.5])
+
+        def close(self):
+            pass
+
+    monkeypatch.setattr(serve._lib, "context", lambda device: object())
+    monkeypatch.setattr(serve, "upload_store", lambda store, ctx: None)
+    monkeypatch.setattr(serve, "_Worker", FakeWorker)
+    store = SimpleNamespace(tables=[SimpleNamespace(shape=(87, 49, 200, 219))] * 3)
+    bank = lambda name: SimpleNamespace(name=name, u=np.zeros(16), n_time=16384, W=np.zeros((16, 100)))
+    srv = serve.Server(store, {"good": bank("good"), "bad": bank("bad")}, hbm_budget=1 << 40, max_workers=2)
+    reqs = [serve.Request(0, "bad", None, seed=3), serve.Request(1, "good", None, seed=4),
+            serve.Request(2, "good", None, seed=5)]
+    srv.serve(reqs)
+    with pytest.raises(MemoryError, match="no room"):
+        reqs[0].future.result(timeout=0)
+    assert [r.future.result(timeout=0)[1] for r in reqs[1:]] == [1.5, 1.5]
+    assert srv.n_created == 1 and srv.sched.n_workers() == 1
+    assert srv.sched.used == 10                           # the good worker's measured size only
+    assert not srv.sched.busy
