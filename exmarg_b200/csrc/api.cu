@@ -427,9 +427,12 @@ extern "C" void exm_ctx_destroy(exm_ctx *ctx)
     if (free_parent) ctx_free(free_parent);
 }
 
-// the calling thread's last failure on a context (by the address of its message), and its last read
-static thread_local const exm_errmsg *tl_err_owner = nullptr;
+// the calling thread's last failure on a context (by the id of its message), and its last read
+static std::atomic<uint64_t> g_errmsg_ids{1};
+static thread_local uint64_t tl_err_owner = 0;
 static thread_local std::string tl_err_msg, tl_err_read;
+
+exm_errmsg::exm_errmsg() : id_(g_errmsg_ids.fetch_add(1)) {}
 
 exm_errmsg &exm_errmsg::operator=(const std::string &m)
 {
@@ -437,7 +440,7 @@ exm_errmsg &exm_errmsg::operator=(const std::string &m)
         std::lock_guard<std::mutex> lk(mu_);
         msg_ = m;
     }
-    tl_err_owner = this;
+    tl_err_owner = id_;
     tl_err_msg = m;
     return *this;
 }
@@ -450,7 +453,7 @@ exm_errmsg::operator std::string() const
 
 const char *exm_errmsg::c_str() const
 {
-    if (tl_err_owner == this) {
+    if (tl_err_owner == id_) {
         tl_err_read = tl_err_msg;
     } else {
         std::lock_guard<std::mutex> lk(mu_);

@@ -87,9 +87,12 @@ struct exm_errmsg {
     operator std::string() const;   // the context's latest message (a copy)
     const char *c_str() const;      // as described above; valid until this thread's next c_str()
 
+    exm_errmsg();
+
   private:
     mutable std::mutex mu_;
     std::string msg_;
+    uint64_t id_;   // unique over the process's lifetime (a context made at a freed one's address gets a new id)
 };
 
 struct exm_ctx {
